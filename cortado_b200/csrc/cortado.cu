@@ -1,0 +1,601 @@
+// libcortado: the C-ABI drop-in for the reference's encode/decode path.
+// Declarations and the reference entry point each function replaces are in
+// include/cortado.h.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <float.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "../../include/cortado.h"
+#include "kernels.cuh"
+
+using namespace cortado;
+
+// ================================================================== kernels
+namespace {
+
+__device__ __forceinline__ Smem& smem_block() {
+  extern __shared__ uint8_t smem_raw[];
+  return *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+}
+
+// Last CTA out resets the chunk queue for the next launch on this context.
+__device__ __forceinline__ void finish_launch(const Sync& sy) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&sy.counter[1], 1u) == gridDim.x - 1) {
+      sy.counter[0] = 0;
+      sy.counter[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+// Loads the full-chunk float words of group g from a swizzled buffer.
+__device__ __forceinline__ void load_plain_rows(uint32_t* buf, const uint8_t* src, long long c, int nw) {
+  const uint32_t* g = reinterpret_cast<const uint32_t*>(src) + c * (long long)CW;
+  for (int w = threadIdx.x; w < CW; w += NT) buf[swz(w)] = (w < nw) ? g[w] : 0u;
+}
+
+struct StreamHdr {
+  long long n, chunks;
+  int eb_e;
+  bool ok;
+};
+
+__device__ __forceinline__ StreamHdr read_header(const uint8_t* s, long long bytes) {
+  StreamHdr h;
+  h.ok = bytes >= HDR;
+  h.n = h.ok ? *reinterpret_cast<const long long*>(s) : 0;
+  h.eb_e = h.ok ? *reinterpret_cast<const int*>(s + 8) : 1;
+  h.ok = h.ok && h.n >= 0 && (h.n & 3) == 0 && h.eb_e >= 1 && h.eb_e <= 230;
+  h.chunks = h.ok ? (h.n + CS - 1) / CS : 0;
+  h.ok = h.ok && (HDR + 2 * h.chunks <= bytes);
+  if (!h.ok) h.chunks = 0;
+  return h;
+}
+
+// ---- store (d_server_encode_kernel)
+__global__ void __launch_bounds__(NT) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
+  Smem& sm = smem_block();
+  const int tid = threadIdx.x;
+  const long long n = a.n;
+  const long long chunks = (n + CS - 1) / CS;
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    *reinterpret_cast<long long*>(a.out) = n;
+    reinterpret_cast<int*>(a.out)[2] = a.q1.eb_e;
+    reinterpret_cast<int*>(a.out)[3] = 0;
+    if (chunks == 0) *a.out_size = HDR;
+  }
+  __syncthreads();
+  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
+  uint8_t* data = a.out + HDR + 2 * chunks;
+  uint32_t phase = 0;
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= chunks) break;
+    const int nw = (int)min((long long)CW, (n - c * CS) / 4);
+    if (nw == CW && a.has_map_in) {
+      if (tid == 0) {
+        fence_proxy_async();
+        mbar_expect_tx(&sm.bar, CS);
+        tma_load_rows(sm.buf0, &map_in, (int)(c * 128), &sm.bar);
+      }
+      if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
+      phase ^= 1;
+    } else {
+      load_plain_rows(sm.buf0, a.in, c, nw);
+      __syncthreads();
+    }
+    uint32_t v[32];
+    row_load(sm.buf0, tid, v);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
+    encode_chunk(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    __syncthreads();
+  }
+  finish_launch(a.sy);
+}
+
+// ---- init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel)
+template <int OP>
+__global__ void __launch_bounds__(NT) k_reencode(const __grid_constant__ OpArgs a) {
+  Smem& sm = smem_block();
+  const int tid = threadIdx.x;
+  const StreamHdr h = read_header(a.in, a.in_bytes);
+  const bool hdr_ok = h.ok && h.n == a.n;
+  const long long chunks = hdr_ok ? h.chunks : 0;
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
+    const long long n = hdr_ok ? h.n : 0;
+    *reinterpret_cast<long long*>(a.out) = n;
+    reinterpret_cast<int*>(a.out)[2] = (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e;
+    reinterpret_cast<int*>(a.out)[3] = 0;
+    if (chunks == 0) *a.out_size = HDR;
+  }
+  __syncthreads();
+  const Quant qs = make_quant(h.eb_e);
+  const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
+  const uint8_t* din = a.in + HDR + 2 * chunks;
+  const long long dbytes = a.in_bytes - HDR - 2 * chunks;
+  uint16_t* tout = reinterpret_cast<uint16_t*>(a.out + HDR);
+  uint8_t* dout = a.out + HDR + 2 * chunks;
+  DecState ds{0, 0, 0};
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= chunks) break;
+    const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
+    uint32_t v[32];
+    bool raw;
+    decode_chunk(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
+    // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
+    // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+      if (OP == OP_S2C) {
+        v[k] = cq_enc(x, a.q1);
+      } else {
+        const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, a.q1), a.q1), a.q2);
+        v[k] = cq_enc(x, a.q2) - src_req;
+      }
+    }
+    row_store(sm.buf0, tid, v);  // raw source: the bins / residuals
+    encode_chunk(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
+    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    __syncthreads();
+  }
+  finish_launch(a.sy);
+}
+
+// ---- storage decode / init_recv / resi_recv
+template <int OP>
+__global__ void __launch_bounds__(NT) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
+                                               const __grid_constant__ CUtensorMap map_out) {
+  Smem& sm = smem_block();
+  const int tid = threadIdx.x;
+  const StreamHdr h = read_header(a.in, a.in_bytes);
+  bool hdr_ok = h.ok && h.n <= a.out_cap;
+  if (OP == OP_RAPPLY) hdr_ok = hdr_ok && h.n == a.n;
+  const long long chunks = hdr_ok ? h.chunks : 0;
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
+    *a.out_size = hdr_ok ? h.n : 0;
+  }
+  __syncthreads();
+  const Quant q = make_quant(h.eb_e);
+  const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
+  const uint8_t* din = a.in + HDR + 2 * chunks;
+  const long long dbytes = a.in_bytes - HDR - 2 * chunks;
+  uint32_t* outbuf = (OP == OP_RAPPLY) ? sm_src(sm) : sm.buf0;
+  DecState ds{0, 0, 0};
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= chunks) break;
+    const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
+    const bool full = nw == CW;
+    uint32_t v[32];
+    bool raw;
+    const bool tma_src = (OP == OP_RAPPLY) && full && a.has_map_in;
+    if (OP == OP_RAPPLY && !tma_src) load_plain_rows(sm_src(sm), a.src, c, nw);
+    decode_chunk(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
+    if (OP == OP_RAPPLY) {
+      // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
+      // destination bound, add the residual, dequantize.
+      uint32_t s[32];
+      row_load(sm_src(sm), tid, s);
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s[k], q) + v[k], q);
+    } else if (OP == OP_SDEC || !raw) {
+      // storage decode always dequantizes; init_recv copies raw chunks out
+      // as stored (d_client_encode.h:230-254)
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
+    }
+    row_store(outbuf, tid, v);
+    if (full && a.has_map_out) {
+      fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        tma_store_rows(&map_out, (int)(c * 128), outbuf);
+        bulk_commit();
+      }
+    } else {
+      __syncthreads();
+      uint32_t* g = reinterpret_cast<uint32_t*>(a.out) + c * (long long)CW;
+      for (int w = tid; w < nw; w += NT) g[w] = outbuf[swz(w)];
+    }
+    if (tid == 0) {
+      if (OP == OP_RAPPLY) bulk_wait_read();  // buf2 is reloaded by the next chunk
+      sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) bulk_wait_read();
+  finish_launch(a.sy);
+}
+
+// ---- NOA range: min/max over the floats, NaNs ignored
+__global__ void k_minmax(const float* x, long long nw, unsigned int* out /* [2]: ordered-int min, max */) {
+  float mn = INFINITY, mx = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  auto ord = [](float f) -> unsigned int {
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  };
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], ord(mn));
+    atomicMax(&out[1], ord(mx));
+  }
+}
+
+}  // namespace
+
+// ================================================================== host side
+struct cortado_ctx {
+  int device = 0;
+  int sms = 0;
+  int grid_store = 0, grid_reenc = 0, grid_dec = 0, grid_rapply = 0;
+  unsigned long long* flags = nullptr;
+  long long flags_cap = 0;
+  unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax
+  unsigned int epoch = 0;
+  unsigned long long timeout_ns = 2000000000ull;
+};
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// A float array viewed as rows of 128 bytes, loaded/stored one chunk (128 rows)
+// at a time with the 128-byte swizzle.
+bool make_rows_map(CUtensorMap* m, const void* base, long long n_bytes) {
+  memset(m, 0, sizeof(*m));
+  const long long rows = n_bytes / 128;
+  if (rows < 128) return false;
+  auto fn = tmap_encoder();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {32, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {128};
+  cuuint32_t box[2] = {32, 128};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cortado_status from_cuda(cudaError_t e) { return e == cudaSuccess ? CORTADO_OK : (e == cudaErrorMemoryAllocation ? CORTADO_ERR_OOM : CORTADO_ERR_CUDA); }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+int64_t chunks_of(int64_t n) { return (n + CS - 1) / CS; }
+
+cortado_status eb_exponent(float eb, int* e) {
+  if (!(eb >= FLT_MIN)) return (eb != eb) ? CORTADO_ERR_EB_TOO_LARGE : CORTADO_ERR_EB_TOO_SMALL;
+  uint32_t bits;
+  memcpy(&bits, &eb, 4);
+  const int be = (int)((bits >> 23) & 0xff);
+  if (be + 24 >= 255) return CORTADO_ERR_EB_TOO_LARGE;
+  *e = be;
+  return CORTADO_OK;
+}
+
+cortado_status ensure_flags(cortado_ctx* ctx, int64_t chunks, cudaStream_t st) {
+  if (chunks <= ctx->flags_cap) return CORTADO_OK;
+  long long cap = 1024;
+  while (cap < chunks) cap *= 2;
+  if (ctx->flags) {
+    cudaStreamSynchronize(st);
+    cudaFree(ctx->flags);
+    ctx->flags = nullptr;
+    ctx->flags_cap = 0;
+  }
+  cudaError_t e = cudaMalloc(&ctx->flags, (size_t)cap * 8);
+  if (e != cudaSuccess) return from_cuda(e);
+  e = cudaMemsetAsync(ctx->flags, 0, (size_t)cap * 8, st);
+  if (e != cudaSuccess) return from_cuda(e);
+  ctx->flags_cap = cap;
+  ctx->epoch = 0;
+  return CORTADO_OK;
+}
+
+Sync next_sync(cortado_ctx* ctx, cudaStream_t st) {
+  if (++ctx->epoch >= 65536u) {
+    cudaMemsetAsync(ctx->flags, 0, (size_t)ctx->flags_cap * 8, st);
+    ctx->epoch = 1;
+  }
+  Sync s;
+  s.flags = ctx->flags;
+  s.counter = ctx->words;
+  s.status = ctx->words + 2;
+  s.epoch = ctx->epoch;
+  s.timeout_ns = ctx->timeout_ns;
+  return s;
+}
+
+int grid_for(int per_sm_grid, int64_t chunks) {
+  long long g = chunks < 1 ? 1 : chunks;
+  return (int)(g < per_sm_grid ? g : per_sm_grid);
+}
+
+template <typename K>
+int occupancy_grid(K kernel, size_t smem, int sms) {
+  int per = 0;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NT, smem);
+  if (per < 1) per = 1;
+  return per * sms;
+}
+
+constexpr size_t SMEM_STD = SMEM_BYTES + 1024;           // + alignment slack
+constexpr size_t SMEM_SRC = SMEM_BYTES + CS + 1024;      // resi_recv: + client chunk
+
+cortado_status launch_status(cudaError_t e) { return from_cuda(e == cudaSuccess ? cudaGetLastError() : e); }
+
+}  // namespace
+
+extern "C" {
+
+const char* cortado_status_string(cortado_status s) {
+  switch (s) {
+    case CORTADO_OK: return "ok";
+    case CORTADO_ERR_EB_TOO_SMALL: return "error bound too small";
+    case CORTADO_ERR_EB_TOO_LARGE: return "error bound too large";
+    case CORTADO_ERR_CORRUPT_STREAM: return "corrupt stream";
+    case CORTADO_ERR_SIZE_MISMATCH: return "size mismatch";
+    case CORTADO_ERR_TIMEOUT: return "device wait timed out";
+    case CORTADO_ERR_OOM: return "out of device memory";
+    case CORTADO_ERR_INVALID_ARG: return "invalid argument";
+    case CORTADO_ERR_CUDA: return "CUDA error";
+    case CORTADO_ERR_ALIGNMENT: return "buffer not 16-byte aligned";
+    case CORTADO_ERR_CAPACITY: return "output buffer too small";
+  }
+  return "unknown status";
+}
+
+int64_t cortado_max_stream_bytes(int64_t n_bytes) {
+  if (n_bytes < 0) return -1;
+  const int64_t c = chunks_of(n_bytes);
+  return HDR + 2 * c + c * (int64_t)CS;
+}
+
+cortado_status cortado_eb_exponent(float eb, int* biased_exponent) {
+  int e = 0;
+  const cortado_status s = eb_exponent(eb, &e);
+  if (s == CORTADO_OK && biased_exponent) *biased_exponent = e;
+  return s;
+}
+
+cortado_status cortado_create(cortado_ctx** out, int device) {
+  if (!out) return CORTADO_ERR_INVALID_ARG;
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return from_cuda(e);
+  cortado_ctx* ctx = new cortado_ctx();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  e = cudaMalloc(&ctx->words, 64);
+  if (e != cudaSuccess) { delete ctx; return from_cuda(e); }
+  cudaMemset(ctx->words, 0, 64);
+  ctx->grid_store = occupancy_grid(k_store, SMEM_STD, ctx->sms);
+  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
+  ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
+  ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_SRC, ctx->sms);
+  cortado_status s = ensure_flags(ctx, 1024, 0);
+  cudaDeviceSynchronize();
+  if (s != CORTADO_OK) { cortado_destroy(ctx); return s; }
+  *out = ctx;
+  return from_cuda(cudaGetLastError());
+}
+
+void cortado_destroy(cortado_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  cudaFree(ctx->flags);
+  cudaFree(ctx->words);
+  delete ctx;
+}
+
+cortado_status cortado_set_timeout(cortado_ctx* ctx, uint64_t timeout_ns) {
+  if (!ctx || timeout_ns == 0) return CORTADO_ERR_INVALID_ARG;
+  ctx->timeout_ns = timeout_ns;
+  return CORTADO_OK;
+}
+
+cortado_status cortado_sync(cortado_ctx* ctx, cortado_stream_t stream) {
+  if (!ctx) return CORTADO_ERR_INVALID_ARG;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return from_cuda(e);
+  unsigned int st = 0;
+  e = cudaMemcpy(&st, ctx->words + 2, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return from_cuda(e);
+  if (st) cudaMemset(ctx->words + 2, 0, 4);
+  return (cortado_status)st;
+}
+
+cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float eb_abs, void* d_out,
+                                    int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream) {
+  if (!ctx || (!d_in && n_bytes) || !d_out || !d_outsize || n_bytes < 0 || (n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
+  if (!aligned16(d_in) || !aligned16(d_out)) return CORTADO_ERR_ALIGNMENT;
+  if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
+  int e = 0;
+  cortado_status s = eb_exponent(eb_abs / 2, &e);  // stored bins use half the bound
+  if (s) return s;
+  const int64_t chunks = chunks_of(n_bytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((s = ensure_flags(ctx, chunks, st))) return s;
+  OpArgs a{};
+  a.in = (const uint8_t*)d_in;
+  a.in_bytes = n_bytes;
+  a.out = (uint8_t*)d_out;
+  a.out_cap = out_capacity;
+  a.out_size = (long long*)d_outsize;
+  a.n = n_bytes;
+  a.q1 = make_quant(e);
+  a.sy = next_sync(ctx, st);
+  CUtensorMap map;
+  a.has_map_in = make_rows_map(&map, d_in, n_bytes);
+  k_store<<<grid_for(ctx->grid_store, chunks), NT, SMEM_STD, st>>>(a, map);
+  return launch_status(cudaSuccess);
+}
+
+static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                               float eb1, float eb2, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                               cortado_stream_t stream) {
+  if (!ctx || !d_stored || !d_out || !d_outsize || n_bytes < 0 || (n_bytes & 3) || stored_bytes < HDR)
+    return CORTADO_ERR_INVALID_ARG;
+  if (!aligned16(d_stored) || !aligned16(d_out)) return CORTADO_ERR_ALIGNMENT;
+  if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
+  int e1 = 0, e2 = 0;
+  cortado_status s = eb_exponent(eb1, &e1);
+  if (s) return s;
+  if (op == OP_RESI && (s = eb_exponent(eb2, &e2))) return s;
+  const int64_t chunks = chunks_of(n_bytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((s = ensure_flags(ctx, chunks, st))) return s;
+  OpArgs a{};
+  a.in = (const uint8_t*)d_stored;
+  a.in_bytes = stored_bytes;
+  a.out = (uint8_t*)d_out;
+  a.out_cap = out_capacity;
+  a.out_size = (long long*)d_outsize;
+  a.n = n_bytes;
+  a.q1 = make_quant(e1);
+  a.q2 = make_quant(e2);
+  a.sy = next_sync(ctx, st);
+  const int grid = grid_for(ctx->grid_reenc, chunks);
+  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
+  else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
+  return launch_status(cudaSuccess);
+}
+
+cortado_status cortado_init_send(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                 float request_eb_abs, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                 cortado_stream_t stream) {
+  return reencode(ctx, OP_S2C, d_stored, stored_bytes, n_bytes, request_eb_abs, 0.0f, d_out, out_capacity, d_outsize, stream);
+}
+
+cortado_status cortado_resi_send(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                 float src_eb_abs, float dst_eb_abs, void* d_out, int64_t out_capacity,
+                                 int64_t* d_outsize, cortado_stream_t stream) {
+  return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_abs, dst_eb_abs, d_out, out_capacity, d_outsize,
+                  stream);
+}
+
+static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int64_t stream_bytes, const void* d_src,
+                             int64_t n_bytes, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                             cortado_stream_t stream) {
+  if (!ctx || !d_stream || !d_out || !d_outsize || stream_bytes < HDR || out_capacity < 0) return CORTADO_ERR_INVALID_ARG;
+  if (!aligned16(d_stream) || !aligned16(d_out) || (d_src && !aligned16(d_src))) return CORTADO_ERR_ALIGNMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  OpArgs a{};
+  a.in = (const uint8_t*)d_stream;
+  a.in_bytes = stream_bytes;
+  a.src = (const uint8_t*)d_src;
+  a.out = (uint8_t*)d_out;
+  a.out_cap = out_capacity;
+  a.out_size = (long long*)d_outsize;
+  a.n = n_bytes;
+  a.sy = next_sync(ctx, st);
+  CUtensorMap msrc, mout;
+  memset(&msrc, 0, sizeof(msrc));
+  // The output map needs the decoded size, which only the stream header holds:
+  // cover the whole output capacity (TMA is only used for full chunks, which
+  // the kernel checks lie inside the header's size).
+  a.has_map_out = make_rows_map(&mout, d_out, op == OP_RAPPLY ? n_bytes : out_capacity);
+  if (op == OP_RAPPLY) a.has_map_in = make_rows_map(&msrc, d_src, n_bytes);
+  const int64_t chunk_bound = chunks_of(op == OP_RAPPLY ? n_bytes : out_capacity);
+  if (op == OP_SDEC) k_decode<OP_SDEC><<<grid_for(ctx->grid_dec, chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
+  else if (op == OP_CDEC) k_decode<OP_CDEC><<<grid_for(ctx->grid_dec, chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
+  else k_decode<OP_RAPPLY><<<grid_for(ctx->grid_rapply, chunk_bound), NT, SMEM_SRC, st>>>(a, msrc, mout);
+  return launch_status(cudaSuccess);
+}
+
+cortado_status cortado_store_decode(cortado_ctx* ctx, const void* d_stream, int64_t stream_bytes, void* d_out,
+                                    int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream) {
+  return decode(ctx, OP_SDEC, d_stream, stream_bytes, nullptr, 0, d_out, out_capacity, d_outsize, stream);
+}
+
+cortado_status cortado_init_recv(cortado_ctx* ctx, const void* d_init, int64_t init_bytes, void* d_out,
+                                 int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream) {
+  return decode(ctx, OP_CDEC, d_init, init_bytes, nullptr, 0, d_out, out_capacity, d_outsize, stream);
+}
+
+cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_bytes, const void* d_resi,
+                                 int64_t resi_bytes, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                 cortado_stream_t stream) {
+  if (!d_src && n_bytes) return CORTADO_ERR_INVALID_ARG;
+  if (n_bytes < 0 || (n_bytes & 3) || out_capacity < n_bytes) return n_bytes < 0 || (n_bytes & 3) ? CORTADO_ERR_INVALID_ARG : CORTADO_ERR_CAPACITY;
+  return decode(ctx, OP_RAPPLY, d_resi, resi_bytes, d_src, n_bytes, d_out, out_capacity, d_outsize, stream);
+}
+
+cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
+                                 cortado_stream_t stream) {
+  if (!ctx || !d_in || !h_min || !h_max || n_bytes <= 0 || (n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned int init[2] = {0xffffffffu, 0u};
+  cudaError_t e = cudaMemcpyAsync(ctx->words + 3, init, 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return from_cuda(e);
+  const long long nw = n_bytes / 4;
+  long long blocks = (nw + 255) / 256;
+  if (blocks > 4L * ctx->sms) blocks = 4L * ctx->sms;
+  k_minmax<<<(int)blocks, 256, 0, st>>>((const float*)d_in, nw, ctx->words + 3);
+  unsigned int r[2];
+  e = cudaMemcpyAsync(r, ctx->words + 3, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return from_cuda(e);
+  auto unord = [](unsigned int o) -> float {
+    const unsigned int u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+  };
+  *h_min = unord(r[0]);
+  *h_max = unord(r[1]);
+  return CORTADO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+// Device building blocks of the B200 Cortado pipeline (sm_100a).
+//
+// Work unit: one 16 KiB chunk (4096 32-bit words) per 128-thread CTA, the
+// reference's format constant CS (include/consts.h:43).  Two register layouts
+// are used:
+//   * group layout   -- thread g holds the 32 consecutive words 32g..32g+31;
+//                       quantizers, DIFFMS and the BIT_4 transpose run here
+//                       without any cross-thread traffic;
+//   * segment layout -- thread t holds the 32 consecutive words 32t..32t+31
+//                       of the BIT_4 output (128 bytes of one bit plane for a
+//                       full chunk); zero elimination, repetition elimination
+//                       and compaction run here, with one block scan.
+// A 16 KiB shared-memory "plane buffer" (128-byte rows, 16-byte units XOR-
+// swizzled by row, the same pattern TMA's 128B swizzle writes) moves words
+// between the layouts without bank conflicts.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cortado {
+
+constexpr int CS = 16384;   // chunk bytes (format constant)
+constexpr int CW = CS / 4;  // chunk words
+constexpr int NT = 128;     // threads per CTA
+constexpr int HDR = 16;     // stream header bytes
+
+// Device-latched status codes (same values as cortado_status).
+enum : uint32_t {
+  DST_OK = 0,
+  DST_CORRUPT = 3,
+  DST_SIZE_MISMATCH = 4,
+  DST_TIMEOUT = 5,
+  DST_CAPACITY = 10,
+};
+
+// Quantizer parameters derived from an error bound's biased exponent
+// (include/d_server_encode.h:150-158).
+struct Quant {
+  int eb_e, thr_e, offs;
+};
+
+__host__ __device__ inline Quant make_quant(int eb_e) {
+  Quant q;
+  q.eb_e = eb_e;
+  q.thr_e = eb_e + 24;
+  q.offs = (q.thr_e << 23) - (1 << 23);
+  return q;
+}
+
+// Per-launch bookkeeping shared by all CTAs (lives in the context workspace).
+struct Sync {
+  unsigned long long* flags;  // lookback words, one per chunk (encoders)
+  unsigned int* counter;      // [0] chunk queue, [1] CTAs finished
+  unsigned int* status;       // first error latched
+  unsigned int epoch;         // 1..65535, tags this launch's lookback words
+  unsigned long long timeout_ns;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t shr_clamp(uint32_t x, uint32_t s) {
+  uint32_t r;
+  asm("shr.b32 %0, %1, %2;" : "=r"(r) : "r"(x), "r"(s));  // s >= 32 gives 0
+  return r;
+}
+__device__ __forceinline__ uint32_t shl_clamp(uint32_t x, uint32_t s) {
+  uint32_t r;
+  asm("shl.b32 %0, %1, %2;" : "=r"(r) : "r"(x), "r"(s));
+  return r;
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Waits for the phase with the given parity to complete; gives up (returns
+// false) after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns) {
+  const uint32_t a = smem_u32(bar);
+  uint32_t done = 0;
+  unsigned long long t0 = 0;
+  for (int it = 0;; ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it == 0) t0 = globaltimer();
+    else if ((it & 63) == 0 && globaltimer() - t0 > limit_ns) return false;
+  }
+}
+// 2-D tiled TMA load of a 32x128 uint32 box (one chunk, 128 rows of 128 B).
+__device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int row, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_rows(const CUtensorMap* map, int row, const void* src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(0), "r"(row), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// 1-D bulk copy global -> shared (16-byte aligned addresses and size).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ---------------------------------------------------------------- status
+__device__ __forceinline__ void latch(unsigned int* status, unsigned int code) {
+  atomicCAS(status, 0u, code);
+}
+
+// ---------------------------------------------------------------- quantizers
+// Server quantizer (truncation), include/components/d_SQ_IABS_4.h:62-76.
+// Values below the bound's exponent give shift >= 25, which the clamping
+// shift turns into 0, so no separate test is needed.
+__device__ __forceinline__ uint32_t sq_enc(uint32_t v, const Quant& q) {
+  const uint32_t a = v & 0x7fffffffu;
+  const int ve = (int)(a >> 23);
+  const uint32_t mant = (v & 0x7fffffu) | 0x800000u;
+  const uint32_t lossy = shr_clamp(mant, (uint32_t)(q.thr_e - ve));
+  const uint32_t enc = (ve >= q.thr_e) ? a - (uint32_t)q.offs : lossy;
+  const uint32_t s = (uint32_t)((int32_t)v >> 31);
+  return (enc ^ s) - s;
+}
+// Client quantizer (round half away from zero), d_CQ_IABS_4.h:62-77.
+__device__ __forceinline__ uint32_t cq_enc(uint32_t v, const Quant& q) {
+  const uint32_t a = v & 0x7fffffffu;
+  const int ve = (int)(a >> 23);
+  const uint32_t sh = (uint32_t)(q.thr_e - ve);
+  const uint32_t mant = (v & 0x7fffffu) | 0x800000u;
+  const uint32_t lossy = shr_clamp(mant + shl_clamp(1u, sh - 1u), sh);
+  const uint32_t enc = (ve >= q.thr_e) ? a - (uint32_t)q.offs : lossy;
+  const uint32_t s = (uint32_t)((int32_t)v >> 31);
+  return (enc ^ s) - s;
+}
+// Dequantizer shared by server and client bins, d_SQ_IABS_4.h:90-107.
+__device__ __forceinline__ uint32_t iq_dec(uint32_t enc, const Quant& q) {
+  const uint32_t neg = (uint32_t)((int32_t)enc >> 31);
+  const uint32_t a = (enc ^ neg) - neg;
+  const int sh = __clz(a) - 8;
+  const uint32_t lossy = ((a << (sh & 31)) & 0x7fffffu) | ((uint32_t)(q.thr_e - sh) << 23);
+  uint32_t dec = (a >= 0x800000u) ? a + (uint32_t)q.offs : lossy;
+  dec |= enc & 0x80000000u;
+  return enc ? dec : 0u;
+}
+
+// ---------------------------------------------------------------- BIT_4
+// The reference's BIT_4 warp butterfly (include/components/d_BIT_4.h:41-92)
+// maps input word i, bit b of a 32-word group to output plane 31-b, bit 31-i:
+// the MSB-first 32x32 bit transpose.  Here it is done in-thread with the
+// recursive block-swap transpose (H. S. Warren, Hacker's Delight, 2nd ed.,
+// sec. 7-3); the 16- and 8-bit stages are byte permutes.  The transform is an
+// involution, so the decoder applies the same function.
+template <int J>
+__device__ __forceinline__ void swap_stage(uint32_t (&a)[32], uint32_t m) {
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    const int k = (i / J) * 2 * J + (i % J);
+    const uint32_t t = (a[k] ^ (a[k + J] >> J)) & m;
+    a[k] ^= t;
+    a[k + J] ^= t << J;
+  }
+}
+__device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    const uint32_t x = a[k], y = a[k + 16];
+    a[k] = __byte_perm(x, y, 0x3276);
+    a[k + 16] = __byte_perm(x, y, 0x1054);
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    const int k = (i / 8) * 16 + (i % 8);
+    const uint32_t x = a[k], y = a[k + 8];
+    a[k] = __byte_perm(x, y, 0x3715);
+    a[k + 8] = __byte_perm(x, y, 0x2604);
+  }
+  swap_stage<4>(a, 0x0F0F0F0Fu);
+  swap_stage<2>(a, 0x33333333u);
+  swap_stage<1>(a, 0x55555555u);
+}
+
+// ---------------------------------------------------------------- byte masks
+// 4-bit mask of the non-zero bytes of x (bit b <-> byte b).
+__device__ __forceinline__ uint32_t nz_nibble(uint32_t x) {
+  const uint32_t h = (((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u;
+  return ((h >> 7) * 0x01020408u) >> 24;
+}
+// Byte-permute selector that scatters the first popc(m) bytes of a word to
+// the positions of the set bits of m and zero-fills the others.
+__device__ __forceinline__ uint32_t expand_sel(uint32_t m) {
+  const uint32_t s = (m | (m << 3) | (m << 6) | (m << 9)) & 0x1111u;
+  const uint32_t r = s * 0x1110u;
+  return (r | ((s ^ 0x1111u) << 2)) & 0xffffu;
+}
+
+// ---------------------------------------------------------------- swizzle
+// Linear word index -> physical word index in a 1024-byte-aligned 16 KiB
+// buffer of 128-byte rows whose 16-byte units are XOR-ed with (row % 8)
+// (identical to CU_TENSOR_MAP_SWIZZLE_128B).
+__device__ __forceinline__ uint32_t swz(uint32_t w) {
+  const uint32_t row = w >> 5;
+  return (row << 5) | ((((w >> 2) & 7u) ^ (row & 7u)) << 2) | (w & 3u);
+}
+// Reads / writes one 128-byte row (32 words) of a swizzled buffer.
+__device__ __forceinline__ void row_load(const uint32_t* buf, int row, uint32_t (&v)[32]) {
+  const uint4* r = reinterpret_cast<const uint4*>(buf + row * 32);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const uint4 u = r[k ^ (row & 7)];
+    v[4 * k] = u.x;
+    v[4 * k + 1] = u.y;
+    v[4 * k + 2] = u.z;
+    v[4 * k + 3] = u.w;
+  }
+}
+__device__ __forceinline__ void row_store(uint32_t* buf, int row, const uint32_t (&v)[32]) {
+  uint4* r = reinterpret_cast<uint4*>(buf + row * 32);
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k ^ (row & 7)] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+// ---------------------------------------------------------------- scans
+// Exclusive scan over the 128 threads of a CTA; tmp holds 4 words and must not
+// be reused by another scan until a later barrier.
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t v, uint32_t* tmp, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) tmp[warp] = x;
+  __syncthreads();
+  const uint32_t w0 = tmp[0], w1 = tmp[1], w2 = tmp[2], w3 = tmp[3];
+  total = w0 + w1 + w2 + w3;
+  const uint32_t pre = (warp > 0 ? w0 : 0u) + (warp > 1 ? w1 : 0u) + (warp > 2 ? w2 : 0u);
+  return pre + x - v;
+}
+__device__ __forceinline__ uint32_t warp_scan_excl(uint32_t v, uint32_t& total) {
+  const int lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------- lookback
+// Lookback word: [63:48] launch epoch, [47:46] state (1 aggregate, 2 inclusive),
+// [45:0] byte count.
+constexpr unsigned long long LB_AGG = 1ull << 46, LB_INC = 2ull << 46, LB_VAL = (1ull << 46) - 1;
+
+// Decoupled lookback over the chunk sizes (the role of propagate_carry,
+// include/d_compression.h:120-160).  Called by one whole warp; returns the
+// exclusive prefix of compressed bytes before chunk c.  Every wait is bounded:
+// on timeout, or when another CTA has already failed, the launch's status is
+// set and 0 is returned.
+__device__ __forceinline__ unsigned long long lookback(const Sync& sy, long long c, unsigned int csize) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long tag = (unsigned long long)sy.epoch << 48;
+  if (lane == 0) st_relaxed(&sy.flags[c], tag | (c == 0 ? LB_INC : LB_AGG) | csize);
+  if (c == 0) return 0;
+  unsigned long long excl = 0;
+  long long top = c - 1;
+  const unsigned long long t0 = globaltimer();
+  while (true) {
+    const long long idx = top - lane;
+    unsigned long long f = 0;
+    bool ready;
+    int spins = 0;
+    while (true) {
+      f = (idx >= 0) ? ld_relaxed(&sy.flags[idx]) : (tag | LB_INC);
+      ready = ((f >> 48) == sy.epoch) && ((f & (3ull << 46)) != 0);
+      if (__all_sync(0xffffffffu, ready)) break;
+      if ((++spins & 31) == 0) {
+        int bad = 0;
+        if (lane == 0) bad = (globaltimer() - t0 > sy.timeout_ns) || (*(volatile unsigned int*)sy.status != 0);
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        if (bad) {
+          if (lane == 0) latch(sy.status, DST_TIMEOUT);
+          return 0;
+        }
+      }
+    }
+    const unsigned int inc = __ballot_sync(0xffffffffu, (f & LB_INC) != 0);
+    if (inc) {
+      const int p = __ffs(inc) - 1;
+      excl += warp_sum64(lane <= p ? (f & LB_VAL) : 0ull);
+      break;
+    }
+    excl += warp_sum64(f & LB_VAL);
+    top -= 32;
+  }
+  if (lane == 0) st_relaxed(&sy.flags[c], tag | LB_INC | (excl + csize));
+  return excl;
+}
+
+}  // namespace cortado

@@ -1,0 +1,483 @@
+// The fused per-chunk encode and decode stages and the six operations built
+// from them.  Reference counterparts:
+//   store encode   include/d_server_encode.h:51-143
+//   storage decode include/d_server_encode.h:174-260
+//   init_send      include/d_s2c.h:51-200
+//   init_recv      include/d_client_encode.h:173-259
+//   resi_send      include/d_residual_encode.h:51-201
+//   resi_recv      include/d_residual_encode.h:238-347
+// Differences in mechanism (not in output bytes): chunk offsets from a bounded,
+// epoch-tagged decoupled lookback (encoders) or a per-CTA running sum of the
+// size table (decoders); one 128-thread CTA per chunk with the data held in
+// registers; TMA for float chunks and compressed payloads; errors latched in a
+// status word instead of printf + __trap.
+#pragma once
+#include "device.cuh"
+
+namespace cortado {
+
+enum Op : int { OP_STORE = 0, OP_S2C = 1, OP_RESI = 2, OP_SDEC = 3, OP_CDEC = 4, OP_RAPPLY = 5 };
+
+// Shared memory of one CTA.  buf0/buf1 are 16 KiB + slack; buf0 is 1024-byte
+// aligned for TMA's 128B swizzle.
+struct __align__(1024) Smem {
+  uint32_t buf0[CW + 64];  // float chunk (TMA), compressed payload, raw source, output staging
+  uint32_t buf1[CW + 64];  // plane buffer, then compacted output
+  uint16_t l2[NT];         // level-2 bitmap (2 bytes per segment thread)
+  uint32_t rb[NT];         // decoder: RE1 rank base per segment thread
+  uint32_t scan_a[4], scan_b[4], scan_c[4], xchg[4];
+  uint64_t bar;
+  long long chunk, next_chunk;
+  unsigned long long payload_off;
+  uint32_t info[8];
+};
+
+struct OpArgs {
+  const uint8_t* in;        // store: floats; others: input stream
+  long long in_bytes;       // store: N; others: valid bytes of the input stream
+  const uint8_t* src;       // resi_recv: client floats
+  uint8_t* out;             // output stream or floats
+  long long out_cap;
+  long long* out_size;      // device
+  long long n;              // original bytes (host-known for encoders; 0 = read header)
+  Quant q1, q2;             // store: server; init_send: request; resi_send: src, dst
+  Sync sy;
+  int has_map_in, has_map_out;
+};
+
+// resi_recv's third buffer (client source chunk, then output staging) follows
+// the Smem block at the next 1024-byte boundary.
+constexpr size_t SMEM_BYTES = ((sizeof(Smem) + 1023) & ~size_t(1023));
+__device__ __forceinline__ uint32_t* sm_src(Smem& sm) {
+  return reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(&sm) + SMEM_BYTES);
+}
+
+// Writes `csize` payload bytes to global memory at dst (any alignment) with
+// 16-byte stores for the aligned interior.  word(q) returns payload word q
+// (bytes 4q..4q+3, little-endian).
+template <typename WordFn>
+__device__ __forceinline__ void store_payload(uint8_t* dst, int csize, WordFn word) {
+  const int tid = threadIdx.x;
+  const uintptr_t A = reinterpret_cast<uintptr_t>(dst);
+  const uintptr_t a0 = (A + 15) & ~uintptr_t(15);
+  const uintptr_t a1 = (A + csize) & ~uintptr_t(15);
+  auto byte_at = [&](int i) -> uint8_t { return (uint8_t)(word(i >> 2) >> (8 * (i & 3))); };
+  if (a1 > a0) {
+    const int head = (int)(a0 - A);
+    const int nblk = (int)((a1 - a0) >> 4);
+    const int r = head & 3;
+    for (int b = tid; b < nblk; b += NT) {
+      const int o = head + 16 * b;
+      const int q = o >> 2;
+      uint32_t w0 = word(q), w1 = word(q + 1), w2 = word(q + 2), w3 = word(q + 3);
+      if (r) {
+        const uint32_t w4 = word(q + 4);
+        w0 = __funnelshift_r(w0, w1, 8 * r);
+        w1 = __funnelshift_r(w1, w2, 8 * r);
+        w2 = __funnelshift_r(w2, w3, 8 * r);
+        w3 = __funnelshift_r(w3, w4, 8 * r);
+      }
+      *reinterpret_cast<uint4*>(a0 + 16 * (uintptr_t)b) = make_uint4(w0, w1, w2, w3);
+    }
+    if (tid < head) dst[tid] = byte_at(tid);
+    const int tail = (int)(A + csize - a1);
+    if (tid < tail) dst[(a1 - A) + tid] = byte_at((int)(a1 - A) + tid);
+  } else {
+    for (int i = tid; i < csize; i += NT) dst[i] = byte_at(i);
+  }
+}
+
+// ============================================================== encode stage
+// Input: v[32] = the pre-DIFFMS words of group g = threadIdx.x (quantized bins
+// or residuals; words at or beyond nw are 0), the raw source (those words in a
+// swizzled buffer, used when the chunk does not compress).  Produces the
+// chunk's payload in the output stream and its size-table entry
+// (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1 -> raw fallback -> carry -> s2g).
+__device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t (&v)[32], const uint32_t* raw_src,
+                                             long long c, int nw, long long chunks, uint8_t* data_out,
+                                             uint16_t* table_out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int osize = nw * 4;
+  const int G = nw >> 5, rem = nw & 31;
+
+  // DIFFMS (d_DIFFMS.h:44-66): word minus its predecessor, then zig-zag.
+  if (lane == 31) sm.xchg[warp] = v[31];
+  __syncthreads();
+  uint32_t prev = __shfl_up_sync(0xffffffffu, v[31], 1);
+  if (lane == 0) prev = warp ? sm.xchg[warp - 1] : 0u;
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    const uint32_t cur = v[k];
+    const uint32_t d = cur - prev;
+    prev = cur;
+    v[k] = (d << 1) ^ (uint32_t)((int32_t)d >> 31);
+  }
+  if (32 * tid + 32 > nw) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (32 * tid + k >= nw) v[k] = 0;
+  }
+  // BIT_4: full groups are transposed into the planes (plane s at linear
+  // words s*G .. s*G+G-1); the trailing partial group is copied untransposed.
+  uint32_t* plane = sm.buf1;
+  if (tid < G) {
+    transpose32(v);
+#pragma unroll
+    for (int s = 0; s < 32; s++) plane[swz(s * G + tid)] = v[s];
+  } else if (tid == G && rem) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (k < rem) plane[swz(32 * G + k)] = v[k];
+  }
+  __syncthreads();
+
+  // Segment layout: thread t owns BIT-output words 32t..32t+31.
+  uint32_t q[32];
+  row_load(plane, tid, q);
+  if (32 * tid + 32 > nw) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (32 * tid + k >= nw) q[k] = 0;
+  }
+  // Zero-elimination bitmap (d_ZEencodebyteshort): bit i <-> byte i != 0.
+  uint32_t M[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) m |= nz_nibble(q[8 * j + i]) << (4 * i);
+    M[j] = m;
+  }
+  const uint32_t nz = __popc(M[0]) + __popc(M[1]) + __popc(M[2]) + __popc(M[3]);
+  // Last bitmap byte of the previous segment (RE's predecessor of byte 0).
+  uint32_t pb = 0;
+  if (tid > 0) {
+    const int w = 32 * tid - 2;
+    const uint32_t x0 = (w < nw) ? plane[swz(w)] : 0u;
+    const uint32_t x1 = (w + 1 < nw) ? plane[swz(w + 1)] : 0u;
+    pb = nz_nibble(x0) | (nz_nibble(x1) << 4);
+  }
+  // Repetition elimination, level 1 (d_REencode4wordsperthread): keep bitmap
+  // byte j iff it differs from byte j-1.
+  uint32_t K = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const uint32_t sh = (M[j] << 8) | (j ? (M[j - 1] >> 24) : pb);
+    K |= nz_nibble(M[j] ^ sh) << (4 * j);
+  }
+  const uint32_t c1 = __popc(K);
+  sm.l2[tid] = (uint16_t)K;
+  uint32_t tot;
+  const uint32_t ex = block_scan_excl(nz | (c1 << 16), sm.scan_a, tot);
+  const uint32_t NZ = tot & 0xffffu, C1 = tot >> 16;
+  const uint32_t zoff = ex & 0xffffu, c1off = ex >> 16;
+  // (barrier inside the scan: the plane buffer is now free -> staging)
+  uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf1);
+
+  if (warp == 0) {
+    // Levels 2 and 3 and the top bitmap (d_REencode1wordperthread), one warp.
+    const uint2 b2 = reinterpret_cast<const uint2*>(sm.l2)[lane];
+    const uint32_t pprev = __shfl_up_sync(0xffffffffu, b2.y >> 24, 1);
+    const uint32_t p0 = lane ? pprev : 0u;
+    const uint32_t k2 = nz_nibble(b2.x ^ ((b2.x << 8) | p0)) | (nz_nibble(b2.y ^ ((b2.y << 8) | (b2.x >> 24))) << 4);
+    uint32_t C2;
+    const uint32_t off2 = warp_scan_excl(__popc(k2), C2);
+    const uint32_t p3 = __shfl_up_sync(0xffffffffu, k2, 1);
+    const bool keep3 = k2 != (lane ? p3 : 0u);
+    const uint32_t top = __ballot_sync(0xffffffffu, keep3);
+    const uint32_t C3 = __popc(top);
+    const uint32_t off3 = __popc(top & ((1u << lane) - 1u));
+    const uint32_t T = NZ + C1 + C2 + C3;
+    unsigned int csize = (NZ == 0) ? 2u : T + 6u;
+    const bool raw = csize >= (unsigned)osize;
+    if (raw) csize = osize;
+    const unsigned long long X = lookback(a.sy, c, csize);
+    if (lane == 0) {
+      sm.info[0] = csize;
+      sm.info[1] = raw;
+      sm.payload_off = X;
+    }
+    if (!raw) {
+      if (NZ == 0) {
+        if (lane == 0) {
+          st[0] = (uint8_t)osize;
+          st[1] = (uint8_t)(osize >> 8);
+        }
+      } else {
+        uint32_t p = NZ + C1 + off2;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          if ((k2 >> j) & 1) st[p++] = (uint8_t)((j < 4 ? b2.x : b2.y) >> (8 * (j & 3)));
+        if (keep3) st[NZ + C1 + C2 + off3] = (uint8_t)k2;
+        if (lane < 4) st[T + lane] = (uint8_t)(top >> (8 * lane));
+        if (lane == 4) st[T + 4] = (uint8_t)osize;
+        if (lane == 5) st[T + 5] = (uint8_t)(osize >> 8);
+      }
+    }
+  }
+  // Compaction of the zero-eliminated bytes and the kept level-1 bitmap bytes
+  // (all warps; the result is discarded if warp 0 decides the chunk is raw).
+  // Skipped when ZE + RE1 alone already reach the chunk size: the chunk is
+  // then certainly raw, and the writes could run past the staging buffer.
+  const bool fits = NZ + C1 + 6 < (uint32_t)osize;
+  if (nz && fits) {
+    uint32_t p = zoff;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const uint32_t m = (M[k >> 3] >> (4 * (k & 7))) & 15u;
+      if (m == 15u) {
+        st[p] = (uint8_t)q[k];
+        st[p + 1] = (uint8_t)(q[k] >> 8);
+        st[p + 2] = (uint8_t)(q[k] >> 16);
+        st[p + 3] = (uint8_t)(q[k] >> 24);
+        p += 4;
+      } else if (m) {
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+          if ((m >> b) & 1) st[p++] = (uint8_t)(q[k] >> (8 * b));
+      }
+    }
+  }
+  if (K && fits) {
+    uint32_t p = NZ + c1off;
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+      if ((K >> j) & 1) st[p++] = (uint8_t)(M[j >> 2] >> (8 * (j & 3)));
+  }
+  __syncthreads();
+  const unsigned int csize = sm.info[0];
+  const bool raw = sm.info[1];
+  const unsigned long long X = sm.payload_off;
+  if (raw) {
+    store_payload(data_out + X, csize, [&](int w) -> uint32_t { return w < nw ? raw_src[swz(w)] : 0u; });
+  } else {
+    store_payload(data_out + X, csize, [&](int w) -> uint32_t { return sm.buf1[w]; });
+  }
+  if (tid == 0) {
+    table_out[c] = (uint16_t)csize;
+    if (c == chunks - 1) *a.out_size = HDR + 2 * chunks + (long long)(X + csize);
+  }
+}
+
+// ============================================================== decode stage
+// Finds chunk c's payload (running sum of the size table, as the reference's
+// decoders do, d_s2c.h:98-106), loads it with a TMA bulk copy, undoes RZE_1,
+// BIT_4 and DIFFMS, and returns the pre-pipeline words of group
+// g = threadIdx.x in v[32] (words at or beyond nw are 0).  *raw reports a chunk
+// stored uncompressed (its words are returned as stored).
+struct DecState {
+  long long prev_c;
+  unsigned long long prev_off;
+  uint32_t phase;
+};
+
+__device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw,
+                                             long long chunks, const uint16_t* table, const uint8_t* data_in,
+                                             long long data_bytes, uint32_t (&v)[32], bool& raw_out,
+                                             const CUtensorMap* src_map, int src_row) {
+  const bool also_src = src_map != nullptr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int osize = nw * 4;
+  const int G = nw >> 5, rem = nw & 31;
+  uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf0);
+
+  // Payload offset: warp 0 sums the size-table entries since its last chunk.
+  if (warp == 0) {
+    unsigned long long s = 0;
+    for (long long i = ds.prev_c + lane; i < c; i += 32) s += table[i];
+    s = warp_sum64(s);
+    ds.prev_off += s;
+    ds.prev_c = c;
+    if (lane == 0) {
+      const int cs = table[c];
+      const long long off = (long long)ds.prev_off;
+      int bad = (cs > osize) || (cs < 2 && cs != osize) || (off + cs > data_bytes);
+      sm.info[0] = bad ? 0u : (uint32_t)cs;
+      sm.info[1] = bad;
+      sm.payload_off = off;
+      // TMA: 16-byte-aligned interior of the payload; the ragged tail by hand.
+      const uintptr_t A = reinterpret_cast<uintptr_t>(data_in + off);
+      const uintptr_t a0 = A & ~uintptr_t(15);
+      uintptr_t a1 = (A + (bad ? 0 : cs)) & ~uintptr_t(15);
+      if (a1 < a0) a1 = a0;
+      sm.info[2] = (uint32_t)(A - a0);
+      sm.info[3] = (uint32_t)(a1 - a0);
+      uint32_t tx = (uint32_t)(a1 - a0) + (also_src ? (uint32_t)CS : 0u);
+      bulk_wait_read();  // a previous TMA store may still be reading buf0
+      fence_proxy_async();
+      if (tx) {
+        mbar_expect_tx(&sm.bar, tx);
+        if (a1 > a0) bulk_load(st, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), &sm.bar);
+        if (also_src) tma_load_rows(sm_src(sm), src_map, src_row, &sm.bar);
+      }
+      sm.info[4] = tx != 0;
+    }
+  }
+  __syncthreads();
+  const int csize = (int)sm.info[0];
+  const int d = (int)sm.info[2];
+  const int tma_len = (int)sm.info[3];
+  {
+    const uint8_t* g = data_in + sm.payload_off;
+    const int from = tma_len - d;  // payload bytes [from, csize) are loaded by hand
+    for (int i = tid + (from > 0 ? from : 0); i < csize; i += NT) st[d + i] = g[i];
+  }
+  if (sm.info[4]) {
+    if (!mbar_wait(&sm.bar, ds.phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
+    ds.phase ^= 1;
+  }
+  __syncthreads();
+  raw_out = false;
+  if (sm.info[1]) {  // corrupt size entry
+    if (tid == 0) latch(a.sy.status, DST_CORRUPT);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = 0;
+    return;
+  }
+  if (csize == osize) {
+    // Stored uncompressed: realign the payload words into the plane buffer.
+    raw_out = true;
+    for (int w = tid; w < nw; w += NT) {
+      const int o = d + 4 * w;
+      const uint32_t lo = sm.buf0[o >> 2], hi = sm.buf0[(o >> 2) + 1];
+      sm.buf1[swz(w)] = __funnelshift_r(lo, hi, 8 * (o & 3));
+    }
+    __syncthreads();
+    row_load(sm.buf1, tid, v);
+    if (32 * tid + 32 > nw) {
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+        if (32 * tid + k >= nw) v[k] = 0;
+    }
+    return;
+  }
+  // ---- undo RZE_1 (d_iRZE, d_RZE.h:127-206)
+  bool ok = true;
+  const int orig = st[d + csize - 2] | (st[d + csize - 1] << 8);
+  ok = (orig == osize);
+  uint32_t M[4] = {0, 0, 0, 0};
+  uint32_t zbase = 0;
+  if (csize == 2) {
+    // all-zero BIT_4 output
+  } else {
+    const int T = csize - 6;
+    if (warp == 0) {
+      bool wok = T >= 0;
+      const int Tc = T < 0 ? 0 : T;
+      const uint32_t top = (uint32_t)st[d + Tc] | ((uint32_t)st[d + Tc + 1] << 8) | ((uint32_t)st[d + Tc + 2] << 16) |
+                           ((uint32_t)st[d + Tc + 3] << 24);
+      const int c3 = __popc(top);
+      wok = wok && (c3 <= T);
+      const int b3 = Tc - c3;
+      const int r3 = __popc(top & (0xffffffffu >> (31 - lane))) - 1;
+      const uint32_t l3 = (r3 >= 0 && wok) ? st[d + b3 + r3] : 0u;
+      uint32_t c2u;
+      const uint32_t e2 = warp_scan_excl(__popc(l3), c2u);
+      const int c2 = (int)c2u;
+      wok = wok && (c3 + c2 <= T);
+      const int b2 = b3 - c2;
+      uint32_t l2lo = 0, l2hi = 0;
+      uint8_t prevb = 0;
+      if (wok && e2 > 0) prevb = st[d + b2 + e2 - 1];
+      uint32_t rk = e2;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if ((l3 >> j) & 1) prevb = wok ? st[d + b2 + rk++] : 0;
+        if (j < 4) l2lo |= (uint32_t)prevb << (8 * j);
+        else l2hi |= (uint32_t)prevb << (8 * (j - 4));
+      }
+      reinterpret_cast<uint2*>(sm.l2)[lane] = make_uint2(l2lo, l2hi);
+      // RE1 rank base for segment threads 4*lane .. 4*lane+3.
+      const uint32_t p0 = __popc(l2lo & 0xffffu), p1 = __popc(l2lo >> 16), p2 = __popc(l2hi & 0xffffu);
+      const uint32_t p3 = __popc(l2hi >> 16);
+      uint32_t c1u;
+      const uint32_t e1 = warp_scan_excl(p0 + p1 + p2 + p3, c1u);
+      sm.rb[4 * lane] = e1;
+      sm.rb[4 * lane + 1] = e1 + p0;
+      sm.rb[4 * lane + 2] = e1 + p0 + p1;
+      sm.rb[4 * lane + 3] = e1 + p0 + p1 + p2;
+      const int c1 = (int)c1u;
+      wok = wok && (c3 + c2 + c1 <= T);
+      if (lane == 0) {
+        sm.info[5] = wok ? (uint32_t)(b2 - c1) : 0u;  // start of RE1 data = count of ZE bytes
+        sm.info[6] = wok;
+      }
+    }
+    __syncthreads();
+    const bool wok = sm.info[6];
+    ok = ok && wok;
+    zbase = sm.info[5];
+    if (wok) {
+      const uint32_t Kb = sm.l2[tid];
+      uint32_t rk = sm.rb[tid];
+      uint8_t prevb = rk > 0 ? st[d + zbase + rk - 1] : 0;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        if ((Kb >> j) & 1) prevb = st[d + zbase + rk++];
+        M[j >> 2] |= (uint32_t)prevb << (8 * (j & 3));
+      }
+    }
+  }
+  // bitmap bits beyond the chunk must be clear
+  if (32 * tid + 32 > nw) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (32 * tid + k >= nw) {
+        const uint32_t bm = 15u << (4 * (k & 7));
+        if (M[k >> 3] & bm) ok = false;
+        M[k >> 3] &= ~bm;
+      }
+  }
+  const uint32_t nz = __popc(M[0]) + __popc(M[1]) + __popc(M[2]) + __popc(M[3]);
+  uint32_t NZ;
+  const uint32_t zoff = block_scan_excl(nz, sm.scan_b, NZ);
+  if (csize != 2 && NZ != zbase) ok = false;
+  if (csize == 2 && NZ != 0) ok = false;
+  if (!ok) latch(a.sy.status, DST_CORRUPT);
+  // ZE decode: scatter the non-zero bytes back into the 32 words.
+  uint32_t q[32];
+  {
+    uint32_t p = (uint32_t)d + (ok ? zoff : 0u);
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const uint32_t m = ok ? (M[k >> 3] >> (4 * (k & 7))) & 15u : 0u;
+      uint32_t x = 0;
+      if (m) {
+        const uint32_t lo = sm.buf0[p >> 2], hi = sm.buf0[(p >> 2) + 1];
+        x = __byte_perm(__funnelshift_r(lo, hi, 8 * (p & 3)), 0u, expand_sel(m));
+        p += __popc(m);
+      }
+      q[k] = x;
+    }
+  }
+  row_store(sm.buf1, tid, q);
+  __syncthreads();
+  // ---- undo BIT_4 (d_iBIT_4): gather plane words of group g, transpose.
+  if (tid < G) {
+#pragma unroll
+    for (int s = 0; s < 32; s++) v[s] = sm.buf1[swz(s * G + tid)];
+    transpose32(v);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = (tid == G && k < rem) ? sm.buf1[swz(32 * G + k)] : 0u;
+  }
+  // ---- undo DIFFMS (d_iDIFFMS, d_DIFFMS.h:69-102): un-zig-zag, prefix sum.
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    const uint32_t z = v[k];
+    acc += (z >> 1) ^ (0u - (z & 1u));
+    v[k] = acc;
+  }
+  uint32_t dummy;
+  const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] += carry;
+  if (32 * tid + 32 > nw) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (32 * tid + k >= nw) v[k] = 0;
+  }
+}
+
+}  // namespace cortado

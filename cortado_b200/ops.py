@@ -1,0 +1,188 @@
+"""Host mirror of the reference's operator interface for the encode/decode path.
+
+The reference exposes header-only host wrappers that take device buffers
+(include/d_server_encode.h:146 ``d_server_encode``, :263 ``d_server_decode``,
+include/d_s2c.h:203 ``d_s2c_encode``, include/d_client_encode.h:262
+``d_client_decode``, include/d_residual_encode.h:204 ``d_residual_encode``,
+:350 ``d_residual_apply``, include/preprocessors/include/INOA_f32.h:52
+``d_INOA_find_range``).  ``Codec`` offers the same operations with the same
+argument meaning on torch CUDA tensors, calling libcortado's C ABI:
+
+* bounds are absolute float32 values (the callers do the NOA scaling, as the
+  reference's CLIs do); ``server_encode`` halves its bound for the stored bins;
+* output sizes are written to a device int64 (``d_outsize``), as in the
+  reference;
+* error-bound problems raise ``CortadoError`` (the reference throws
+  ``std::runtime_error("LC error")``); problems the device detects are raised by
+  ``sync()`` (the reference traps).
+
+The ``store``/``init_send``/... convenience methods allocate their outputs,
+synchronize and return trimmed tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _native
+from ._native import CortadoError, check
+
+CS = 16384
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _nbytes(t: torch.Tensor) -> int:
+    return t.numel() * t.element_size()
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, torch.cuda.Stream):
+        return stream.cuda_stream
+    return int(stream)
+
+
+def max_stream_bytes(n_bytes: int) -> int:
+    return int(_native.lib().cortado_max_stream_bytes(n_bytes))
+
+
+def eb_exponent(eb_abs: float) -> int:
+    e = ctypes.c_int()
+    check(_native.lib().cortado_eb_exponent(float(eb_abs), ctypes.byref(e)), "error bound")
+    return e.value
+
+
+class Codec:
+    """One libcortado context (scratch for one stream at a time) on a device."""
+
+    def __init__(self, device: int | torch.device | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("cortado_b200 needs a CUDA device")
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = torch.device("cuda", device if isinstance(device, int) else device.index or 0)
+        self._L = _native.lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(self._L.cortado_create(ctypes.byref(h), self.device.index), "cortado_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cortado_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_timeout(self, seconds: float):
+        check(self._L.cortado_set_timeout(self._h, int(seconds * 1e9)), "set_timeout")
+
+    def sync(self, stream=None):
+        """Waits for the stream and raises the first device-detected error."""
+        check(self._L.cortado_sync(self._h, _stream(stream)), "device")
+
+    # ------------------------------------------------ reference-shaped operations
+    def server_encode(self, d_input, insize, d_output, d_outsize, eb, stream=None):
+        check(self._L.cortado_store_encode(self._h, _ptr(d_input), int(insize), float(eb), _ptr(d_output),
+                                           _nbytes(d_output), _ptr(d_outsize), _stream(stream)), "server_encode")
+
+    def server_decode(self, d_input, d_output, d_outsize, in_bytes=None, stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_store_decode(self._h, _ptr(d_input), n, _ptr(d_output), _nbytes(d_output),
+                                           _ptr(d_outsize), _stream(stream)), "server_decode")
+
+    def s2c_encode(self, d_input, d_output, d_outsize, request_eb, n_bytes, in_bytes=None, stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_init_send(self._h, _ptr(d_input), n, int(n_bytes), float(request_eb), _ptr(d_output),
+                                        _nbytes(d_output), _ptr(d_outsize), _stream(stream)), "s2c_encode")
+
+    def client_decode(self, d_input, d_output, d_outsize, in_bytes=None, stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_init_recv(self._h, _ptr(d_input), n, _ptr(d_output), _nbytes(d_output),
+                                        _ptr(d_outsize), _stream(stream)), "client_decode")
+
+    def residual_encode(self, d_input, d_output, d_outsize, src_eb, dest_eb, n_bytes, in_bytes=None, stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_resi_send(self._h, _ptr(d_input), n, int(n_bytes), float(src_eb), float(dest_eb),
+                                        _ptr(d_output), _nbytes(d_output), _ptr(d_outsize), _stream(stream)),
+              "residual_encode")
+
+    def residual_apply(self, d_src, srcsize, d_residual, d_dest, d_destsize, resi_bytes=None, stream=None):
+        n = _nbytes(d_residual) if resi_bytes is None else int(resi_bytes)
+        check(self._L.cortado_resi_recv(self._h, _ptr(d_src), int(srcsize), _ptr(d_residual), n, _ptr(d_dest),
+                                        _nbytes(d_dest), _ptr(d_destsize), _stream(stream)), "residual_apply")
+
+    def INOA_find_range(self, d_data, size=None, stream=None):
+        n = _nbytes(d_data) if size is None else int(size)
+        lo, hi = ctypes.c_float(), ctypes.c_float()
+        check(self._L.cortado_noa_range(self._h, _ptr(d_data), n, ctypes.byref(lo), ctypes.byref(hi),
+                                        _stream(stream)), "INOA_find_range")
+        return lo.value, hi.value
+
+    # ------------------------------------------------ convenience forms
+    def _empty_stream(self, n_bytes):
+        return torch.empty(max_stream_bytes(n_bytes), dtype=torch.uint8, device=self.device)
+
+    def _trim(self, buf, size):
+        self.sync()
+        return buf[: int(size.item())]
+
+    def store(self, x: torch.Tensor, eb_abs: float) -> torch.Tensor:
+        x = x.contiguous()
+        out = self._empty_stream(_nbytes(x))
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.server_encode(x, _nbytes(x), out, size, eb_abs)
+        return self._trim(out, size)
+
+    def store_decode(self, stored: torch.Tensor, n_bytes: int | None = None) -> torch.Tensor:
+        n = n_bytes if n_bytes is not None else stream_orig_bytes(stored)
+        out = torch.empty(max(n, 4) // 4, dtype=torch.float32, device=self.device)
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.server_decode(stored, out, size)
+        self.sync()
+        return out[: n // 4]
+
+    def init_send(self, stored: torch.Tensor, request_eb_abs: float, n_bytes: int | None = None) -> torch.Tensor:
+        n = n_bytes if n_bytes is not None else stream_orig_bytes(stored)
+        out = self._empty_stream(n)
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.s2c_encode(stored, out, size, request_eb_abs, n)
+        return self._trim(out, size)
+
+    def init_recv(self, init: torch.Tensor, n_bytes: int | None = None) -> torch.Tensor:
+        n = n_bytes if n_bytes is not None else stream_orig_bytes(init)
+        out = torch.empty(max(n, 4) // 4, dtype=torch.float32, device=self.device)
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.client_decode(init, out, size)
+        self.sync()
+        return out[: n // 4]
+
+    def resi_send(self, stored: torch.Tensor, src_eb_abs: float, dst_eb_abs: float,
+                  n_bytes: int | None = None) -> torch.Tensor:
+        n = n_bytes if n_bytes is not None else stream_orig_bytes(stored)
+        out = self._empty_stream(n)
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.residual_encode(stored, out, size, src_eb_abs, dst_eb_abs, n)
+        return self._trim(out, size)
+
+    def resi_recv(self, src: torch.Tensor, resi: torch.Tensor) -> torch.Tensor:
+        src = src.contiguous()
+        out = torch.empty_like(src, dtype=torch.float32)
+        size = torch.empty(1, dtype=torch.int64, device=self.device)
+        self.residual_apply(src, _nbytes(src), resi, out, size)
+        self.sync()
+        return out
+
+
+def stream_orig_bytes(stream: torch.Tensor) -> int:
+    """Original size from a stream header (reads 8 bytes to the host)."""
+    return int(stream[:8].cpu().view(torch.int64).item())

@@ -1,0 +1,124 @@
+/*
+ * cortado.h -- C ABI of the B200 implementation of Cortado's encode/decode
+ * path (a progressive, error-bounded float32 compressor).
+ *
+ * Each entry point replaces one host wrapper of the reference (cited below by
+ * file:line within the reference project).  Differences from those wrappers:
+ *   - work is enqueued on the caller's CUDA stream and nothing allocates or
+ *     synchronizes on the hot path (the reference allocates and frees its
+ *     carry array inside every call, include/d_server_encode.h:160-165);
+ *   - errors are status codes: argument and error-bound problems are returned
+ *     at once, problems the device detects (corrupt stream, size mismatch,
+ *     a bounded wait that timed out) are latched in the context and returned
+ *     by cortado_sync() -- the reference throws or calls __trap();
+ *   - a context holds all scratch state; one context serves one stream at a
+ *     time (use one context per concurrently used stream);
+ *   - every device buffer must be 16-byte aligned (cudaMalloc's are) and
+ *     every original size a multiple of 4 bytes.
+ * Streams, .stor.meta files and decoded floats are byte-identical to the
+ * reference's, except header bytes 12..15, which the reference leaves
+ * unwritten and which are written as 0 here.
+ *
+ * Sizes are in bytes.  "d_" pointers are device pointers, "h_" host pointers.
+ */
+#ifndef CORTADO_H
+#define CORTADO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* cortado_stream_t; /* same type as cudaStream_t */
+typedef struct cortado_ctx cortado_ctx;
+
+typedef enum {
+  CORTADO_OK = 0,
+  CORTADO_ERR_EB_TOO_SMALL = 1,   /* bound below FLT_MIN after the reference's adjustments */
+  CORTADO_ERR_EB_TOO_LARGE = 2,   /* bound exponent + 24 reaches the float exponent limit */
+  CORTADO_ERR_CORRUPT_STREAM = 3, /* malformed header, size table or chunk */
+  CORTADO_ERR_SIZE_MISMATCH = 4,  /* stream size differs from the given original size */
+  CORTADO_ERR_TIMEOUT = 5,        /* a bounded device wait gave up */
+  CORTADO_ERR_OOM = 6,
+  CORTADO_ERR_INVALID_ARG = 7,
+  CORTADO_ERR_CUDA = 8,
+  CORTADO_ERR_ALIGNMENT = 9,
+  CORTADO_ERR_CAPACITY = 10       /* output buffer smaller than required */
+} cortado_status;
+
+/* Chunk size of the format (reference include/consts.h:43). */
+#define CORTADO_CHUNK_BYTES 16384
+
+const char* cortado_status_string(cortado_status s);
+
+/* Worst-case stream size for n_bytes of input: 16 + 2*chunks + 16384*chunks
+ * (reference src/cortado_store.cu:196-198). */
+int64_t cortado_max_stream_bytes(int64_t n_bytes);
+
+/* Validates an absolute error bound and returns its biased float exponent,
+ * the only part of a bound that reaches a stream
+ * (reference include/d_server_encode.h:150-158). */
+cortado_status cortado_eb_exponent(float eb_abs, int* biased_exponent);
+
+/* Context: scratch (lookback words, chunk queue, status word) on `device`. */
+cortado_status cortado_create(cortado_ctx** ctx, int device);
+void cortado_destroy(cortado_ctx* ctx);
+/* Upper bound of every device-side wait (default 2 s). */
+cortado_status cortado_set_timeout(cortado_ctx* ctx, uint64_t timeout_ns);
+/* Waits for `stream`, then returns (and clears) the first error the device
+ * latched since the previous call. */
+cortado_status cortado_sync(cortado_ctx* ctx, cortado_stream_t stream);
+
+/* store: encodes n_bytes of float32 at the absolute bound eb_abs (stored bins
+ * use eb_abs/2).  Replaces d_server_encode, include/d_server_encode.h:146-166.
+ * out_capacity >= cortado_max_stream_bytes(n_bytes); *d_outsize receives the
+ * stream length. */
+cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float eb_abs,
+                                    void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                    cortado_stream_t stream);
+
+/* storage decode: stored stream -> floats.  Replaces d_server_decode,
+ * include/d_server_encode.h:263-267.  stream_bytes bounds the reads;
+ * *d_outsize receives the decoded length (from the stream header). */
+cortado_status cortado_store_decode(cortado_ctx* ctx, const void* d_stream, int64_t stream_bytes, void* d_out,
+                                    int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream);
+
+/* init_send: requantizes a stored stream to request_eb_abs and encodes it.
+ * Replaces d_s2c_encode, include/d_s2c.h:203-224.  n_bytes is the original
+ * size (the stored stream's header value; the reference passes the chunk
+ * count). */
+cortado_status cortado_init_send(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                 float request_eb_abs, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                 cortado_stream_t stream);
+
+/* init_recv: decodes an init stream to floats.  Replaces d_client_decode,
+ * include/d_client_encode.h:262-266.  Chunks the encoder stored uncompressed
+ * are copied out as stored, as the reference does. */
+cortado_status cortado_init_recv(cortado_ctx* ctx, const void* d_init, int64_t init_bytes, void* d_out,
+                                 int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream);
+
+/* resi_send: residual between the client's current bound src_eb_abs and the
+ * finer dst_eb_abs, from a stored stream.  Replaces d_residual_encode,
+ * include/d_residual_encode.h:204-230. */
+cortado_status cortado_resi_send(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                 float src_eb_abs, float dst_eb_abs, void* d_out, int64_t out_capacity,
+                                 int64_t* d_outsize, cortado_stream_t stream);
+
+/* resi_recv: applies a residual stream to the client's current floats.
+ * Replaces d_residual_apply, include/d_residual_encode.h:350-354 (the size
+ * check of :257 becomes CORTADO_ERR_SIZE_MISMATCH). */
+cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_bytes, const void* d_resi,
+                                 int64_t resi_bytes, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                 cortado_stream_t stream);
+
+/* NOA range: min and max of the floats (NaNs ignored), synchronous.
+ * Replaces d_INOA_find_range, include/preprocessors/include/INOA_f32.h:52-61. */
+cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
+                                 cortado_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CORTADO_H */

@@ -1,0 +1,109 @@
+"""Shared driver for the golden cases: replays the reference CLI flow
+(store -> init_send -> init_recv -> resi_send -> resi_recv, user mode) for one
+case with a pluggable implementation, and returns the same hash records that
+tests/golden/collect.py extracts from the reference's own outputs."""
+import hashlib
+import json
+import os
+
+import numpy as np
+
+from cortado_b200 import storage
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+C1_SHA256 = "7a5359a5f0df9f34ed4d1b80a797d2f2288d5277fe5e95cd8175cce70d49781f"
+
+
+def stream_hash(b: bytes) -> str:
+    b = bytes(b)
+    if len(b) >= 16:
+        b = b[:12] + b"\0\0\0\0" + b[16:]
+    return hashlib.sha256(b).hexdigest()
+
+
+def file_hash(b) -> str:
+    return hashlib.sha256(bytes(b)).hexdigest()
+
+
+def reference_outputs():
+    with open(os.path.join(GOLDEN, "reference_outputs.json")) as f:
+        return json.load(f)
+
+
+def cases():
+    with open(os.path.join(GOLDEN, "cases.json")) as f:
+        c = json.load(f)
+    out = []
+    for name, settings in sorted(c.items()):
+        for s in settings:
+            out.append((name, s))
+    return out
+
+
+def load_input(name):
+    if name == "c1_sin128":
+        from cortado_b200 import fields
+        x = fields.sinusoid((128, 128, 128), 1).numpy().reshape(-1)
+        if hashlib.sha256(x.tobytes()).hexdigest() != C1_SHA256:
+            return None
+        return x
+    return np.fromfile(os.path.join(GOLDEN, "inputs", name + ".f32"), np.float32)
+
+
+def c1_setting():
+    return {"mode": "noa", "store": ["1e-1", "1e-3", "1e-5"], "init": "1e-2", "resi": ["1e-2", "1e-4"]}
+
+
+class Failed(Exception):
+    pass
+
+
+def run_flow(impl, x: np.ndarray, s: dict):
+    """impl provides: noa_range(x)->(min,max), store(x, eb_abs)->bytes,
+    init_send(stored, n, eb)->bytes, init_recv(stream)->float32 array,
+    resi_send(stored, n, src, dst)->bytes, resi_recv(src_floats, stream)->array.
+    Errors raise; the returned record holds what the reference run produced."""
+    abs_mode = s["mode"] == "abs"
+    rec = {}
+    vmin, vmax = impl.noa_range(x)
+    vrange = storage.value_range(vmin, vmax)
+    _, ebs_abs = storage.store_bounds(s["store"], abs_mode, vrange)
+    try:
+        stor = [impl.store(x, float(e)) for e in ebs_abs]
+    except Exception as err:  # the reference prints an error and aborts
+        rec["store_error"] = str(err)
+        return rec
+    rec["stor"] = {f"{i:02d}": {"sha256": stream_hash(b), "bytes": len(b)} for i, b in enumerate(stor)}
+    rec["meta"] = {"ebs": [int(np.float32(e).view(np.uint32)) for e in ebs_abs],
+                   "range": int(np.float32(vrange).view(np.uint32))}
+    meta = storage.StorMeta("x", ebs_abs, vrange)
+    p = storage.plan_init(meta, s["init"], abs_mode)
+    init = impl.init_send(stor[p.stored_index], x.nbytes, float(p.eb1_abs))
+    rec["init.bin"] = {"sha256": stream_hash(init), "bytes": len(init)}
+    dec = np.ascontiguousarray(impl.init_recv(init), dtype=np.float32)
+    rec["init_dec.f32"] = {"sha256": file_hash(dec.tobytes()), "bytes": dec.nbytes}
+    p = storage.plan_resi(meta, s["resi"][0], s["resi"][1], abs_mode)
+    resi = impl.resi_send(stor[p.stored_index], x.nbytes, float(p.eb1_abs), float(p.eb2_abs))
+    rec["resi.bin"] = {"sha256": stream_hash(resi), "bytes": len(resi)}
+    fin = np.ascontiguousarray(impl.resi_recv(dec, resi), dtype=np.float32)
+    rec["resi_dec.f32"] = {"sha256": file_hash(fin.tobytes()), "bytes": fin.nbytes}
+    rec["_arrays"] = (stor, init, dec, resi, fin, ebs_abs)
+    return rec
+
+
+def compare(rec, ref) -> list:
+    """Differences between an implementation's record and the reference's."""
+    diffs = []
+    if "store_error" in rec or ref["rc"].get("store", 0) != 0:
+        if not ("store_error" in rec and ref["rc"].get("store", 0) != 0):
+            diffs.append(("store outcome", rec.get("store_error"), ref["rc"]))
+        return diffs
+    for k, v in ref["stor"].items():
+        if rec["stor"].get(k) != v:
+            diffs.append(("stor." + k, rec["stor"].get(k), v))
+    if rec["meta"]["ebs"] != ref["meta"]["ebs"] or rec["meta"]["range"] != ref["meta"]["range"]:
+        diffs.append(("meta", rec["meta"], ref["meta"]))
+    for k in ("init.bin", "init_dec.f32", "resi.bin", "resi_dec.f32"):
+        if rec.get(k) != ref.get(k):
+            diffs.append((k, rec.get(k), ref.get(k)))
+    return diffs
