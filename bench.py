@@ -44,9 +44,9 @@ EB_STORE, EB_SRC, EB_DST = "1e-4", "1e-2", "1e-4"
 OPS = ("noa_range", "store", "init_send", "init_recv", "resi_send", "resi_recv")
 
 
-def make_field(seed: int, device) -> torch.Tensor:
+def make_field(seed: int, device, shape=SHAPE) -> torch.Tensor:
     from cortado_b200 import fields
-    return fields.sinusoid(SHAPE, seed, outlier_frac=1e-3, device=device).reshape(-1)
+    return fields.sinusoid(shape, seed, outlier_frac=1e-3, device=device).reshape(-1)
 
 
 def peaks():
@@ -169,7 +169,7 @@ def run_gpu(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     codec = ops.Codec(dev.index)
-    x = make_field(2 + rank, dev)
+    x = make_field(2 + rank, dev, args.shape)
     stream = torch.cuda.Stream(dev)
     fl = Flow(codec, x, stream)
     with torch.cuda.stream(stream):
@@ -236,11 +236,18 @@ def barrier(world):
 
 
 def max_over_ranks(v, world, dev):
+    """Slowest rank's time (every rank takes part; device = the rank's device,
+    or cpu under gloo)."""
     if world == 1:
         return v
     t = torch.tensor([v], dtype=torch.float64, device=dev)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_gbs(field_bytes: int, world: int, ms_per_step: float) -> float:
+    """Whole-job original-data rate: every rank processes its own field."""
+    return world * field_bytes * 1e-9 / (ms_per_step * 1e-3)
 
 
 def load_traffic():
@@ -279,12 +286,14 @@ def main():
     ap.add_argument("--impl", default="cortado_b200", choices=["cortado_b200", "reference"])
     ap.add_argument("--cpu-sample-mb", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="512,512,512", help="field shape (profiling uses a smaller one)")
     args = ap.parse_args()
+    args.shape = tuple(int(v) for v in args.shape.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     cfg = {"workload": "512^3 float32 field (512 MiB), 8 random sinusoids + N(0,1e-3) noise + 0.1% +-1e6 outliers; "
                        "step = NOA range, store 1e-4, init_send 1e-2, init_recv, resi_send 1e-2->1e-4, resi_recv",
-           "field_bytes": 512 ** 3 * 4, "bounds_noa": {"store": EB_STORE, "init": EB_SRC, "resi": [EB_SRC, EB_DST]},
+           "field_bytes": int(np.prod(args.shape)) * 4, "shape": list(args.shape), "bounds_noa": {"store": EB_STORE, "init": EB_SRC, "resi": [EB_SRC, EB_DST]},
            "parallelism": f"replicas{args.gpus} (independent fields, no collective)",
            "l2": "inputs larger than L2 (no flush needed)"}
 
@@ -315,7 +324,7 @@ def main():
     if rank != 0:
         return
     n = r["n"]
-    gbs = world * n * 1e-9 / (r["ms"] * 1e-3)
+    gbs = job_gbs(n, world, r["ms"])
     ops_gbs = {op: (n * 1e-9 / (t * 1e-3) if t > 0 else None) for op, t in zip(OPS, r["per_op"])}
     sizes = r["sizes"]
     s_stor, s_init, s_resi = sizes[0], sizes[1], sizes[3]

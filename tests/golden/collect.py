@@ -2,9 +2,11 @@
 run on a GPU box) into tests/golden/reference_outputs.json: per case and mode,
 the sha256 and size of every stream (header bytes 12..15 zeroed -- the
 reference leaves them unwritten), of every decoded file, the parsed
-.stor.meta fields and the exit codes.
+.stor.meta fields, the exit codes, and -- from four repeated runs of each
+decoder on identical inputs -- every distinct output the decoder produced
+(the reference's resi_recv is not deterministic on some partial last chunks).
 
-Usage: python tests/golden/collect.py <golden-output-dir>
+Usage: python tests/golden/collect.py <golden-output-dir> [more dirs; later ones win]
 """
 import hashlib
 import json
@@ -12,7 +14,29 @@ import os
 import struct
 import sys
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+
+def resi_within_bound(case_dir, name, tag):
+    """MAXABS of the reference's resi_recv output against the original at the
+    destination bound (the reference's own resi_bench -v check)."""
+    from cortado_b200 import storage
+    from oracle import oracle as O
+    cases = json.load(open(os.path.join(HERE, "cases.json")))
+    settings = [s for s in cases.get(name, []) if s["tag"] == tag]
+    inp = os.path.join(HERE, "inputs", name + ".f32")
+    if not settings or not os.path.exists(inp):
+        return None
+    s = settings[0]
+    x = np.fromfile(inp, np.float32)
+    rng = np.float32(1) if s["mode"] == "abs" else O.noa_range(x)
+    dst = storage.f32(s["resi"][1]) if s["mode"] == "abs" else storage.noa_scale(s["resi"][1], rng)
+    out = np.fromfile(os.path.join(case_dir, "resi_dec.f32"), np.float32)
+    return bool(out.size == x.size and O.maxabs(out, x, float(dst)) == -1)
 
 
 def stream_hash(b: bytes) -> str:
@@ -34,7 +58,16 @@ def parse_meta(b: bytes):
             "range": struct.unpack("<I", struct.pack("<f", rng))[0], "name": os.path.basename(name)}
 
 
-def main(root):
+def main(roots):
+    out = {}
+    for root in roots:
+        out.update(collect(root))
+    with open(os.path.join(HERE, "reference_outputs.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("collected", len(out), "runs")
+
+
+def collect(root):
     out = {}
     for case in sorted(os.listdir(root)):
         cdir = os.path.join(root, case)
@@ -61,16 +94,22 @@ def main(root):
                 if os.path.exists(p):
                     b = open(p, "rb").read()
                     rec[f] = {"sha256": stream_hash(b) if kind == "s" else file_hash(b), "bytes": len(b)}
+            for dec, f in (("resi_recv", "resi_dec.f32"), ("init_recv", "init_dec.f32")):
+                rp = os.path.join(d, dec + "_repeat.txt")
+                if os.path.exists(rp) and f in rec:
+                    seen = sorted({ln.strip() for ln in open(rp) if ln.strip()} | {rec[f]["sha256"]})
+                    rec[dec + "_variants"] = seen
+                    rec[dec + "_deterministic"] = len(seen) == 1
+            if "resi_dec.f32" in rec:
+                rec["resi_dec_within_bound"] = resi_within_bound(d, case, mode)
             for log in ("store_bench", "init_bench", "resi_bench"):
                 p = os.path.join(d, log + ".log")
                 if os.path.exists(p):
                     t = open(p).read()
                     rec[log + "_verify"] = ("ERROR" not in t) and ("verification passed" in t or log == "store_bench")
             out[f"{case}/{mode}"] = rec
-    with open(os.path.join(HERE, "reference_outputs.json"), "w") as f:
-        json.dump(out, f, indent=1, sort_keys=True)
-    print("collected", len(out), "runs")
+    return out
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    main(sys.argv[1:])

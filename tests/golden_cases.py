@@ -9,6 +9,7 @@ import os
 import numpy as np
 
 from cortado_b200 import storage
+from oracle import oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 C1_SHA256 = "7a5359a5f0df9f34ed4d1b80a797d2f2288d5277fe5e95cd8175cce70d49781f"
@@ -51,7 +52,7 @@ def load_input(name):
 
 
 def c1_setting():
-    return {"mode": "noa", "store": ["1e-1", "1e-3", "1e-5"], "init": "1e-2", "resi": ["1e-2", "1e-4"]}
+    return {"tag": "noa", "mode": "noa", "store": ["1e-1", "1e-3", "1e-5"], "init": "1e-2", "resi": ["1e-2", "1e-4"]}
 
 
 class Failed(Exception):
@@ -62,7 +63,8 @@ def run_flow(impl, x: np.ndarray, s: dict):
     """impl provides: noa_range(x)->(min,max), store(x, eb_abs)->bytes,
     init_send(stored, n, eb)->bytes, init_recv(stream)->float32 array,
     resi_send(stored, n, src, dst)->bytes, resi_recv(src_floats, stream)->array.
-    Errors raise; the returned record holds what the reference run produced."""
+    Errors raise; the returned record holds what the reference run produced
+    (plus private "_" entries used by compare())."""
     abs_mode = s["mode"] == "abs"
     rec = {}
     vmin, vmax = impl.noa_range(x)
@@ -87,6 +89,7 @@ def run_flow(impl, x: np.ndarray, s: dict):
     rec["resi.bin"] = {"sha256": stream_hash(resi), "bytes": len(resi)}
     fin = np.ascontiguousarray(impl.resi_recv(dec, resi), dtype=np.float32)
     rec["resi_dec.f32"] = {"sha256": file_hash(fin.tobytes()), "bytes": fin.nbytes}
+    rec["_resi_within_bound"] = bool(O.maxabs(fin, x, float(p.eb2_abs)) == -1)
     rec["_arrays"] = (stor, init, dec, resi, fin, ebs_abs)
     return rec
 
@@ -103,7 +106,14 @@ def compare(rec, ref) -> list:
             diffs.append(("stor." + k, rec["stor"].get(k), v))
     if rec["meta"]["ebs"] != ref["meta"]["ebs"] or rec["meta"]["range"] != ref["meta"]["range"]:
         diffs.append(("meta", rec["meta"], ref["meta"]))
-    for k in ("init.bin", "init_dec.f32", "resi.bin", "resi_dec.f32"):
+    for k in ("init.bin", "init_dec.f32", "resi.bin"):
         if rec.get(k) != ref.get(k):
             diffs.append((k, rec.get(k), ref.get(k)))
+    if rec.get("resi_dec.f32") != ref.get("resi_dec.f32"):
+        # The reference's resi_recv (d_residual_apply) returns varying or
+        # out-of-bound results on some partial last chunks; there the result
+        # must instead satisfy the bound the reference's resi_bench -v checks.
+        ref_defective = (not ref.get("resi_recv_deterministic", True)) or ref.get("resi_dec_within_bound") is False
+        if not (ref_defective and rec.get("_resi_within_bound")):
+            diffs.append(("resi_dec.f32", rec.get("resi_dec.f32"), ref.get("resi_dec.f32")))
     return diffs

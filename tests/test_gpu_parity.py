@@ -97,7 +97,7 @@ def test_golden_flow_matches_reference(codec, name, setting):
         pytest.skip("no reference record")
     x = G.load_input(name)
     rec = G.run_flow(GpuImpl(codec), x, setting)
-    diffs = [d for d in G.compare(rec, ref) if not (d[0] == "resi_dec.f32" and not ref.get("resi_recv_deterministic", True))]
+    diffs = G.compare(rec, ref)
     assert not diffs, diffs
 
 

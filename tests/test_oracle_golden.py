@@ -32,9 +32,9 @@ REF = G.reference_outputs()
 CASES = [(n, s) for n, s in G.cases()] + [("c1_sin128", G.c1_setting())]
 
 
-@pytest.mark.parametrize("name,setting", CASES, ids=[f"{n}-{s['mode']}-{i}" for i, (n, s) in enumerate(CASES)])
+@pytest.mark.parametrize("name,setting", CASES, ids=[f"{n}-{s['tag']}" for n, s in CASES])
 def test_oracle_matches_reference(name, setting):
-    key = f"{name}/{setting['mode']}"
+    key = f"{name}/{setting['tag']}"
     ref = REF[key]
     x = G.load_input(name)
     if x is None:
