@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcortado.so")
+# CORTADO_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("CORTADO_LIB") or os.path.join(HERE, "libcortado.so")
 
 STATUS_NAMES = {
     0: "OK", 1: "EB_TOO_SMALL", 2: "EB_TOO_LARGE", 3: "CORRUPT_STREAM", 4: "SIZE_MISMATCH",

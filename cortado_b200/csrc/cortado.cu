@@ -16,6 +16,22 @@
 using namespace cortado;
 
 // ================================================================== kernels
+// Resident CTAs per SM each kernel is compiled for (register budget
+// 65536 / (128 * n)).  resi_recv holds a third 16 KiB buffer, so shared memory
+// limits it to 4.
+#ifndef MINB_STORE
+#define MINB_STORE 6
+#endif
+#ifndef MINB_REENC
+#define MINB_REENC 5
+#endif
+#ifndef MINB_DEC
+#define MINB_DEC 6
+#endif
+#ifndef MINB_RAPPLY
+#define MINB_RAPPLY 4
+#endif
+
 namespace {
 
 __device__ __forceinline__ Smem& smem_block() {
@@ -61,7 +77,7 @@ __device__ __forceinline__ StreamHdr read_header(const uint8_t* s, long long byt
 }
 
 // ---- store (d_server_encode_kernel)
-__global__ void __launch_bounds__(NT) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
+__global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
   Smem& sm = smem_block();
   const int tid = threadIdx.x;
   const long long n = a.n;
@@ -101,7 +117,8 @@ __global__ void __launch_bounds__(NT) k_store(const __grid_constant__ OpArgs a, 
     row_load(sm.buf0, tid, v);
 #pragma unroll
     for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
-    encode_chunk(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
     if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
     __syncthreads();
   }
@@ -110,7 +127,7 @@ __global__ void __launch_bounds__(NT) k_store(const __grid_constant__ OpArgs a, 
 
 // ---- init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel)
 template <int OP>
-__global__ void __launch_bounds__(NT) k_reencode(const __grid_constant__ OpArgs a) {
+__global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
   Smem& sm = smem_block();
   const int tid = threadIdx.x;
   const StreamHdr h = read_header(a.in, a.in_bytes);
@@ -143,7 +160,8 @@ __global__ void __launch_bounds__(NT) k_reencode(const __grid_constant__ OpArgs 
     const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
     uint32_t v[32];
     bool raw;
-    decode_chunk(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
+    if (nw == CW) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
+    else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
     // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
     // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
 #pragma unroll
@@ -157,7 +175,8 @@ __global__ void __launch_bounds__(NT) k_reencode(const __grid_constant__ OpArgs 
       }
     }
     row_store(sm.buf0, tid, v);  // raw source: the bins / residuals
-    encode_chunk(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
+    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
+    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
     if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
     __syncthreads();
   }
@@ -166,7 +185,7 @@ __global__ void __launch_bounds__(NT) k_reencode(const __grid_constant__ OpArgs 
 
 // ---- storage decode / init_recv / resi_recv
 template <int OP>
-__global__ void __launch_bounds__(NT) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
+__global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
                                                const __grid_constant__ CUtensorMap map_out) {
   Smem& sm = smem_block();
   const int tid = threadIdx.x;
@@ -199,7 +218,8 @@ __global__ void __launch_bounds__(NT) k_decode(const __grid_constant__ OpArgs a,
     bool raw;
     const bool tma_src = (OP == OP_RAPPLY) && full && a.has_map_in;
     if (OP == OP_RAPPLY && !tma_src) load_plain_rows(sm_src(sm), a.src, c, nw);
-    decode_chunk(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
+    if (full) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
+    else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
     if (OP == OP_RAPPLY) {
       // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
       // destination bound, add the residual, dequantize.
@@ -207,9 +227,10 @@ __global__ void __launch_bounds__(NT) k_decode(const __grid_constant__ OpArgs a,
       row_load(sm_src(sm), tid, s);
 #pragma unroll
       for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s[k], q) + v[k], q);
-    } else if (OP == OP_SDEC || !raw) {
-      // storage decode always dequantizes; init_recv copies raw chunks out
-      // as stored (d_client_encode.h:230-254)
+    } else if (!raw) {
+      // chunks stored uncompressed are copied out as stored: original floats
+      // for storage decode (d_server_encode.h:234-249), request bins for
+      // init_recv (d_client_encode.h:230-254, the reference's behaviour)
 #pragma unroll
       for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
     }
@@ -239,10 +260,17 @@ __global__ void __launch_bounds__(NT) k_decode(const __grid_constant__ OpArgs a,
 // ---- NOA range: min/max over the floats, NaNs ignored
 __global__ void k_minmax(const float* x, long long nw, unsigned int* out /* [2]: ordered-int min, max */) {
   float mn = INFINITY, mx = -INFINITY;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x) {
-    const float v = x[i];
-    mn = fminf(mn, v);
-    mx = fmaxf(mx, v);
+  const long long nv = nw / 4;
+  const float4* x4 = reinterpret_cast<const float4*>(x);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += stride) {
+    const float4 v = x4[i];
+    mn = fminf(fminf(mn, v.x), fminf(v.y, fminf(v.z, v.w)));
+    mx = fmaxf(fmaxf(mx, v.x), fmaxf(v.y, fmaxf(v.z, v.w)));
+  }
+  for (long long i = 4 * nv + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += stride) {
+    mn = fminf(mn, x[i]);
+    mx = fmaxf(mx, x[i]);
   }
   for (int o = 16; o > 0; o >>= 1) {
     mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
@@ -362,6 +390,7 @@ template <typename K>
 int occupancy_grid(K kernel, size_t smem, int sms) {
   int per = 0;
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NT, smem);
   if (per < 1) per = 1;
   return per * sms;
@@ -599,3 +628,4 @@ cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_b
 }
 
 }  // extern "C"
+

@@ -87,16 +87,28 @@ __device__ __forceinline__ void store_payload(uint8_t* dst, int csize, WordFn wo
   }
 }
 
+// Physical plane-buffer word offsets of linear word s*128 + tid for even and
+// odd s (full chunk): the swizzle term depends on s only through its parity,
+// so the 32 plane words of a thread sit at base + 128*s + (s odd ? o : e).
+__device__ __forceinline__ void plane_offsets(int tid, uint32_t& e, uint32_t& o) {
+  const uint32_t lane = tid & 31, warp = tid >> 5;
+  e = 32 * warp + ((((lane >> 2) & 7u) ^ warp) << 2) + (lane & 3);
+  o = 32 * warp + ((((lane >> 2) & 7u) ^ (warp + 4)) << 2) + (lane & 3);
+}
+
 // ============================================================== encode stage
 // Input: v[32] = the pre-DIFFMS words of group g = threadIdx.x (quantized bins
 // or residuals; words at or beyond nw are 0), the raw source (those words in a
 // swizzled buffer, used when the chunk does not compress).  Produces the
 // chunk's payload in the output stream and its size-table entry
 // (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1 -> raw fallback -> carry -> s2g).
+// FULL: a whole 16 KiB chunk (nw == 4096), with compile-time addressing.
+template <bool FULL>
 __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t (&v)[32], const uint32_t* raw_src,
-                                             long long c, int nw, long long chunks, uint8_t* data_out,
+                                             long long c, int nw_in, long long chunks, uint8_t* data_out,
                                              uint16_t* table_out) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nw = FULL ? CW : nw_in;
   const int osize = nw * 4;
   const int G = nw >> 5, rem = nw & 31;
 
@@ -112,7 +124,7 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
     prev = cur;
     v[k] = (d << 1) ^ (uint32_t)((int32_t)d >> 31);
   }
-  if (32 * tid + 32 > nw) {
+  if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
     for (int k = 0; k < 32; k++)
       if (32 * tid + k >= nw) v[k] = 0;
@@ -120,7 +132,13 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   // BIT_4: full groups are transposed into the planes (plane s at linear
   // words s*G .. s*G+G-1); the trailing partial group is copied untransposed.
   uint32_t* plane = sm.buf1;
-  if (tid < G) {
+  if (FULL) {
+    transpose32(v);
+    uint32_t pe, po;
+    plane_offsets(tid, pe, po);
+#pragma unroll
+    for (int s = 0; s < 32; s++) plane[128 * s + ((s & 1) ? po : pe)] = v[s];
+  } else if (tid < G) {
     transpose32(v);
 #pragma unroll
     for (int s = 0; s < 32; s++) plane[swz(s * G + tid)] = v[s];
@@ -134,7 +152,7 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   // Segment layout: thread t owns BIT-output words 32t..32t+31.
   uint32_t q[32];
   row_load(plane, tid, q);
-  if (32 * tid + 32 > nw) {
+  if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
     for (int k = 0; k < 32; k++)
       if (32 * tid + k >= nw) q[k] = 0;
@@ -153,8 +171,8 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   uint32_t pb = 0;
   if (tid > 0) {
     const int w = 32 * tid - 2;
-    const uint32_t x0 = (w < nw) ? plane[swz(w)] : 0u;
-    const uint32_t x1 = (w + 1 < nw) ? plane[swz(w + 1)] : 0u;
+    const uint32_t x0 = (FULL || w < nw) ? plane[swz(w)] : 0u;
+    const uint32_t x1 = (FULL || w + 1 < nw) ? plane[swz(w + 1)] : 0u;
     pb = nz_nibble(x0) | (nz_nibble(x1) << 4);
   }
   // Repetition elimination, level 1 (d_REencode4wordsperthread): keep bitmap
@@ -271,12 +289,14 @@ struct DecState {
   uint32_t phase;
 };
 
-__device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw,
+template <bool FULL>
+__device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw_in,
                                              long long chunks, const uint16_t* table, const uint8_t* data_in,
                                              long long data_bytes, uint32_t (&v)[32], bool& raw_out,
                                              const CUtensorMap* src_map, int src_row) {
   const bool also_src = src_map != nullptr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nw = FULL ? CW : nw_in;
   const int osize = nw * 4;
   const int G = nw >> 5, rem = nw & 31;
   uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf0);
@@ -344,7 +364,7 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     }
     __syncthreads();
     row_load(sm.buf1, tid, v);
-    if (32 * tid + 32 > nw) {
+    if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
       for (int k = 0; k < 32; k++)
         if (32 * tid + k >= nw) v[k] = 0;
@@ -419,7 +439,7 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     }
   }
   // bitmap bits beyond the chunk must be clear
-  if (32 * tid + 32 > nw) {
+  if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
     for (int k = 0; k < 32; k++)
       if (32 * tid + k >= nw) {
@@ -453,7 +473,13 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   row_store(sm.buf1, tid, q);
   __syncthreads();
   // ---- undo BIT_4 (d_iBIT_4): gather plane words of group g, transpose.
-  if (tid < G) {
+  if (FULL) {
+    uint32_t pe, po;
+    plane_offsets(tid, pe, po);
+#pragma unroll
+    for (int s = 0; s < 32; s++) v[s] = sm.buf1[128 * s + ((s & 1) ? po : pe)];
+    transpose32(v);
+  } else if (tid < G) {
 #pragma unroll
     for (int s = 0; s < 32; s++) v[s] = sm.buf1[swz(s * G + tid)];
     transpose32(v);
@@ -473,11 +499,33 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);
 #pragma unroll
   for (int k = 0; k < 32; k++) v[k] += carry;
-  if (32 * tid + 32 > nw) {
+  if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
     for (int k = 0; k < 32; k++)
       if (32 * tid + k >= nw) v[k] = 0;
   }
+}
+
+// The partial last chunk of a stream (at most one per launch) runs out of
+// line, so the full-chunk loop body stays small enough for the instruction
+// caches.  Arrays pass through local memory on this rare path.
+__device__ __noinline__ void encode_chunk_partial(Smem& sm, const OpArgs& a, uint32_t* v, const uint32_t* raw_src,
+                                                  long long c, int nw, long long chunks, uint8_t* data_out,
+                                                  uint16_t* table_out) {
+  uint32_t w[32];
+#pragma unroll
+  for (int k = 0; k < 32; k++) w[k] = v[k];
+  encode_chunk<false>(sm, a, w, raw_src, c, nw, chunks, data_out, table_out);
+}
+
+__device__ __noinline__ void decode_chunk_partial(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw,
+                                                  long long chunks, const uint16_t* table, const uint8_t* data_in,
+                                                  long long data_bytes, uint32_t* v, bool& raw_out,
+                                                  const CUtensorMap* src_map, int src_row) {
+  uint32_t w[32];
+  decode_chunk<false>(sm, a, ds, c, nw, chunks, table, data_in, data_bytes, w, raw_out, src_map, src_row);
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = w[k];
 }
 
 }  // namespace cortado
