@@ -14,7 +14,7 @@ LIB_PATH = os.environ.get("CORTADO_LIB") or os.path.join(HERE, "libcortado.so")
 
 STATUS_NAMES = {
     0: "OK", 1: "EB_TOO_SMALL", 2: "EB_TOO_LARGE", 3: "CORRUPT_STREAM", 4: "SIZE_MISMATCH",
-    5: "TIMEOUT", 6: "OOM", 7: "INVALID_ARG", 8: "CUDA", 9: "ALIGNMENT", 10: "CAPACITY",
+    5: "TIMEOUT", 6: "OOM", 7: "INVALID_ARG", 8: "CUDA", 9: "ALIGNMENT", 10: "CAPACITY", 11: "SCRATCH_LIMIT",
 }
 
 # Every symbol include/cortado.h declares, with (restype, argtypes).
@@ -34,6 +34,7 @@ SIGNATURES = {
     "cortado_resi_send": (_int, [_vp, _vp, _i64, _i64, _f32, _f32, _vp, _i64, _vp, _vp]),
     "cortado_resi_recv": (_int, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp]),
     "cortado_noa_range": (_int, [_vp, _vp, _i64, ctypes.POINTER(_f32), ctypes.POINTER(_f32), _vp]),
+    "cortado_store_encode_noalloc": (_int, [_vp, _i64, _f32, _vp, _i64, _vp, _vp]),
 }
 
 

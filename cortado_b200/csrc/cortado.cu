@@ -257,6 +257,76 @@ __global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) 
   finish_launch(a.sy);
 }
 
+// ---- store without allocation (cortado_store_encode_noalloc)
+// Fixed scratch for callers that cannot allocate device memory: one
+// lookback word per chunk for up to CORTADO_NOALLOC_MAX_BYTES of input, then
+// the chunk queue, the finished-CTA count and the status word.  Every GPU that
+// loads the library holds this array until the process exits.
+constexpr long long NOALLOC_CHUNKS = CORTADO_NOALLOC_MAX_BYTES / CS;
+__device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_CHUNKS + 4];
+
+// Same chunk loop as k_store; the last CTA out also reports a device-side
+// error as a negative *out_size (there is no context to read it from) and
+// clears the status word for the next call.
+__global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_constant__ OpArgs a,
+                                                                  const __grid_constant__ CUtensorMap map_in) {
+  Smem& sm = smem_block();
+  const int tid = threadIdx.x;
+  const long long n = a.n;
+  const long long chunks = (n + CS - 1) / CS;
+  if (tid == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    *reinterpret_cast<long long*>(a.out) = n;
+    reinterpret_cast<int*>(a.out)[2] = a.q1.eb_e;
+    reinterpret_cast<int*>(a.out)[3] = 0;
+    if (chunks == 0) *a.out_size = HDR;
+  }
+  __syncthreads();
+  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
+  uint8_t* data = a.out + HDR + 2 * chunks;
+  uint32_t phase = 0;
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= chunks) break;
+    const int nw = (int)min((long long)CW, (n - c * CS) / 4);
+    if (nw == CW && a.has_map_in) {
+      if (tid == 0) {
+        fence_proxy_async();
+        mbar_expect_tx(&sm.bar, CS);
+        tma_load_rows(sm.buf0, &map_in, (int)(c * 128), &sm.bar);
+      }
+      if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
+      phase ^= 1;
+    } else {
+      load_plain_rows(sm.buf0, a.in, c, nw);
+      __syncthreads();
+    }
+    uint32_t v[32];
+    row_load(sm.buf0, tid, v);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
+    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    __syncthreads();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sy.counter[1], 1u) == gridDim.x - 1) {
+      const unsigned int st = atomicExch(a.sy.status, 0u);
+      if (st) *a.out_size = -(long long)st;
+      a.sy.counter[0] = 0;
+      a.sy.counter[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
 // ---- NOA range: min/max over the floats, NaNs ignored
 __global__ void k_minmax(const float* x, long long nw, unsigned int* out /* [2]: ordered-int min, max */) {
   float mn = INFINITY, mx = -INFINITY;
@@ -418,6 +488,7 @@ const char* cortado_status_string(cortado_status s) {
     case CORTADO_ERR_CUDA: return "CUDA error";
     case CORTADO_ERR_ALIGNMENT: return "buffer not 16-byte aligned";
     case CORTADO_ERR_CAPACITY: return "output buffer too small";
+    case CORTADO_ERR_SCRATCH_LIMIT: return "input larger than the fixed scratch of the no-allocation entry point";
   }
   return "unknown status";
 }
@@ -625,6 +696,72 @@ cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_b
   *h_min = unord(r[0]);
   *h_max = unord(r[1]);
   return CORTADO_OK;
+}
+
+// Per-device set-up of the no-allocation entry point: the device address of
+// g_noalloc_scratch, the persistent grid size and the lookback epoch.
+struct NoallocDev {
+  bool ready = false;
+  unsigned long long* scratch = nullptr;
+  int grid = 0;
+  unsigned int epoch = 0;
+};
+static NoallocDev g_noalloc_dev[64];
+static std::mutex g_noalloc_mu;
+
+cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, float eb_abs, void* d_out,
+                                            int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream) {
+  if ((!d_in && n_bytes) || !d_out || !d_outsize || n_bytes < 0 || (n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
+  if (n_bytes > CORTADO_NOALLOC_MAX_BYTES) return CORTADO_ERR_SCRATCH_LIMIT;
+  if (!aligned16(d_in) || !aligned16(d_out)) return CORTADO_ERR_ALIGNMENT;
+  if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
+  int e = 0;
+  cortado_status s = eb_exponent(eb_abs / 2, &e);
+  if (s) return s;
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return from_cuda(ce);
+  if (dev < 0 || dev >= 64) return CORTADO_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  NoallocDev& d = g_noalloc_dev[dev];
+  unsigned int epoch;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!d.ready) {
+      // device `dev` is current here
+      void* p = nullptr;
+      ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (ce != cudaSuccess) return from_cuda(ce);
+      int sms = 0;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      d.grid = occupancy_grid(k_store_noalloc, SMEM_STD, sms);
+      d.scratch = (unsigned long long*)p;
+      d.ready = true;
+    }
+    if (++d.epoch >= 65536u) {
+      ce = cudaMemsetAsync(d.scratch, 0, (size_t)NOALLOC_CHUNKS * 8, st);  // clears old lookback words
+      if (ce != cudaSuccess) return from_cuda(ce);
+      d.epoch = 1;
+    }
+    epoch = d.epoch;
+  }
+  OpArgs a{};
+  a.in = (const uint8_t*)d_in;
+  a.in_bytes = n_bytes;
+  a.out = (uint8_t*)d_out;
+  a.out_cap = out_capacity;
+  a.out_size = (long long*)d_outsize;
+  a.n = n_bytes;
+  a.q1 = make_quant(e);
+  a.sy.flags = d.scratch;
+  a.sy.counter = reinterpret_cast<unsigned int*>(d.scratch + NOALLOC_CHUNKS);
+  a.sy.status = a.sy.counter + 2;
+  a.sy.epoch = epoch;
+  a.sy.timeout_ns = 2000000000ull;
+  CUtensorMap map;
+  a.has_map_in = make_rows_map(&map, d_in, n_bytes);
+  k_store_noalloc<<<grid_for(d.grid, chunks_of(n_bytes)), NT, SMEM_STD, st>>>(a, map);
+  return launch_status(cudaSuccess);
 }
 
 }  // extern "C"

@@ -44,7 +44,8 @@ typedef enum {
   CORTADO_ERR_INVALID_ARG = 7,
   CORTADO_ERR_CUDA = 8,
   CORTADO_ERR_ALIGNMENT = 9,
-  CORTADO_ERR_CAPACITY = 10       /* output buffer smaller than required */
+  CORTADO_ERR_CAPACITY = 10,      /* output buffer smaller than required */
+  CORTADO_ERR_SCRATCH_LIMIT = 11  /* input exceeds cortado_store_encode_noalloc's fixed scratch */
 } cortado_status;
 
 /* Chunk size of the format (reference include/consts.h:43). */
@@ -116,6 +117,33 @@ cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_
  * Replaces d_INOA_find_range, include/preprocessors/include/INOA_f32.h:52-61. */
 cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
                                  cortado_stream_t stream);
+
+/* store without allocating: for callers that cannot call cudaMalloc.
+ *
+ * No counterpart in the reference.  Some callers of this library cannot
+ * allocate device memory when they encode: code running under a host
+ * framework that owns the whole device memory pool (a caching allocator or a
+ * serving process that reserved its memory up front), or code on a real-time
+ * path where an allocation's implicit synchronization is not allowed.  The
+ * context-based cortado_store_encode() allocates its scratch at creation and
+ * grows it for larger inputs; this entry point instead uses a fixed scratch
+ * array compiled into the library (CORTADO_NOALLOC_MAX_BYTES / 16384 lookback
+ * words plus three counters, 512 KiB), which every GPU that loads the library
+ * holds until the process exits.  It calls no cudaMalloc, cudaFree or
+ * allocating library routine.  Inputs and outputs are as for
+ * cortado_store_encode(), on the device current at the call.
+ *   - inputs larger than CORTADO_NOALLOC_MAX_BYTES return
+ *     CORTADO_ERR_SCRATCH_LIMIT;
+ *   - the first call on a device looks up the scratch array's device address
+ *     (cudaGetSymbolAddress) and the launch size; make that first call before
+ *     any stream capture;
+ *   - all calls share the one array, so calls that overlap on the GPU (other
+ *     streams, other host threads) race and give wrong output: serialize them;
+ *   - there is no context to latch device-side errors in: a failed launch
+ *     writes a negative status (-CORTADO_ERR_TIMEOUT) to *d_outsize. */
+#define CORTADO_NOALLOC_MAX_BYTES (1LL << 30)
+cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, float eb_abs, void* d_out,
+                                            int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream);
 
 #ifdef __cplusplus
 }
