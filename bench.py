@@ -41,6 +41,8 @@ METRIC = "original-f32 GB/s end-to-end at NOA 1e-4, batched/served vs plain; p50
 UNIT = "GB/s"
 SHAPE = (512, 512, 512)
 EB_STORE, EB_SRC, EB_DST = "1e-4", "1e-2", "1e-4"
+# the same field's ABS-mode configuration (finest stored bound, init, residual)
+ABS_STORE, ABS_SRC, ABS_DST = "1e-6", "1e-3", "1e-5"
 OPS = ("noa_range", "store", "init_send", "init_recv", "resi_send", "resi_recv")
 
 
@@ -116,9 +118,9 @@ class ClockSampler:
 class Flow:
     """Preallocated buffers and the six calls of one step on one stream."""
 
-    def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream):
+    def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream, abs_mode: bool = False):
         from cortado_b200 import ops
-        self.c, self.x, self.s = codec, x, stream
+        self.c, self.x, self.s, self.abs_mode = codec, x, stream, abs_mode
         dev = x.device
         self.n = x.numel() * 4
         cap = ops.max_stream_bytes(self.n)
@@ -132,7 +134,9 @@ class Flow:
 
     def bounds(self):
         from cortado_b200 import storage
-        lo, hi = self.c.INOA_find_range(self.x, stream=self.s)
+        lo, hi = self.c.INOA_find_range(self.x, stream=self.s)  # run in both modes, as the reference's store does
+        if self.abs_mode:
+            return tuple(float(storage.f32(e)) for e in (ABS_STORE, ABS_SRC, ABS_DST))
         rng = storage.value_range(lo, hi)
         return (float(storage.noa_scale(EB_STORE, rng)), float(storage.noa_scale(EB_SRC, rng)),
                 float(storage.noa_scale(EB_DST, rng)))
@@ -226,7 +230,31 @@ def run_gpu(args, rank, world):
         torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(start.elapsed_time(end) / e_steps, world, dev)
     codec.sync(stream)
-    return dict(ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, clocks=clk.summary(), e2e_ms=e2e_ms,
+
+    # ABS-mode pass over the same field (secondary report)
+    fa = Flow(codec, x, stream, abs_mode=True)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            fa.step()
+        codec.sync(stream)
+        _, _, eb_a = fa.bounds()
+        abs_ok = bool(torch.all((fa.fin - x).abs() <= eb_a))
+        abs_sizes = fa.sizes.cpu().tolist()
+        a_steps = max(1, min(args.steps, 5))
+        a_op = np.zeros(len(OPS))
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        start.record(stream)
+        for _ in range(a_steps):
+            fa.step(timed=True)
+            stream.synchronize()
+            a_op += np.array(fa.op_ms())
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    abs_ms = max_over_ranks(start.elapsed_time(end) / a_steps, world, dev)
+    codec.sync(stream)
+    abs_res = dict(ms=abs_ms, per_op=a_op / a_steps, sizes=abs_sizes, ok=abs_ok)
+    return dict(abs=abs_res, ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, clocks=clk.summary(), e2e_ms=e2e_ms,
                 h2d=n, d2h=s_init + s_resi + n)
 
 
@@ -349,6 +377,13 @@ def main():
         "e2e": {"value": world * n * 1e-9 / (r["e2e_ms"] * 1e-3), "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": args.steps * (len(OPS)),
+        "abs_mode": {"bounds_abs": {"store": ABS_STORE, "init": ABS_SRC, "resi": [ABS_SRC, ABS_DST]},
+                     "value": job_gbs(n, world, r["abs"]["ms"]), "ms_per_step": r["abs"]["ms"],
+                     "bounds_verified": r["abs"]["ok"],
+                     "stream_bytes": {"stor": r["abs"]["sizes"][0], "init": r["abs"]["sizes"][1],
+                                      "resi": r["abs"]["sizes"][3]},
+                     "ops": {k: {"ms": t, "orig_GBps": n * 1e-9 / (t * 1e-3) if t > 0 else None}
+                             for k, t in zip(OPS, r["abs"]["per_op"])}},
         "clocks": r["clocks"],
     }
     if not args.no_cpu_baseline and world == 1:

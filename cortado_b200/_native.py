@@ -35,7 +35,19 @@ SIGNATURES = {
     "cortado_resi_recv": (_int, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp]),
     "cortado_noa_range": (_int, [_vp, _vp, _i64, ctypes.POINTER(_f32), ctypes.POINTER(_f32), _vp]),
     "cortado_store_encode_noalloc": (_int, [_vp, _i64, _f32, _vp, _i64, _vp, _vp]),
+    "cortado_batch": (_int, [_vp, _int, _vp, _int, _vp]),
+    "cortado_verify_bound": (_int, [_vp, _vp, _vp, _i64, _f32, _vp, _vp]),
+    "cortado_set_launch_ctas": (_int, [_vp, _int, _int]),
 }
+
+OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5}
+
+
+class Item(ctypes.Structure):
+    """cortado_item (include/cortado.h)."""
+    _fields_ = [("d_in", ctypes.c_void_p), ("in_bytes", ctypes.c_int64), ("n_bytes", ctypes.c_int64),
+                ("eb1", ctypes.c_float), ("eb2", ctypes.c_float), ("d_src", ctypes.c_void_p),
+                ("d_out", ctypes.c_void_p), ("out_capacity", ctypes.c_int64), ("d_outsize", ctypes.c_void_p)]
 
 
 class CortadoError(RuntimeError):

@@ -39,17 +39,37 @@ __device__ __forceinline__ Smem& smem_block() {
   return *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 }
 
-// Last CTA out resets the chunk queue for the next launch on this context.
-__device__ __forceinline__ void finish_launch(const Sync& sy) {
+// Reads this launch's lookback epoch (every CTA, at start).
+__device__ __forceinline__ void begin_launch(Smem& sm, const Sync& sy) {
+  if (threadIdx.x == 0) sm.epoch = *(volatile unsigned int*)sy.epoch;
+}
+
+// The last CTA out resets the chunk queue and advances the epoch for the next
+// launch on this scratch; when the 16-bit epoch wraps it first clears the
+// lookback words, so no word of an old launch can carry the new epoch.
+// Returns the status word's value to the last CTA's thread 0 (else 0).
+__device__ __forceinline__ unsigned int finish_launch(Smem& sm, const Sync& sy, bool take_status = false) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(&sy.counter[1], 1u) == gridDim.x - 1) {
+    sm.is_last = atomicAdd(&sy.counter[1], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  unsigned int st = 0;
+  if (sm.is_last) {
+    const unsigned int e = sm.epoch;
+    if (e == 65535u)
+      for (long long i = threadIdx.x; i < sy.flags_cap; i += blockDim.x) sy.flags[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (take_status) st = atomicExch(sy.status, 0u);
+      *sy.epoch = (e == 65535u) ? 0u : e + 1u;
       sy.counter[0] = 0;
       sy.counter[1] = 0;
       __threadfence();
     }
   }
+  return st;
 }
 
 // Loads the full-chunk float words of group g from a swizzled buffer.
@@ -76,204 +96,293 @@ __device__ __forceinline__ StreamHdr read_header(const uint8_t* s, long long byt
   return h;
 }
 
-// ---- store (d_server_encode_kernel)
-__global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
-  Smem& sm = smem_block();
-  const int tid = threadIdx.x;
-  const long long n = a.n;
-  const long long chunks = (n + CS - 1) / CS;
-  if (tid == 0) {
-    mbar_init(&sm.bar, 1);
-    fence_mbar_init();
-    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-  }
-  if (blockIdx.x == 0 && tid == 0) {
-    *reinterpret_cast<long long*>(a.out) = n;
-    reinterpret_cast<int*>(a.out)[2] = a.q1.eb_e;
-    reinterpret_cast<int*>(a.out)[3] = 0;
-    if (chunks == 0) *a.out_size = HDR;
-  }
-  __syncthreads();
-  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
-  uint8_t* data = a.out + HDR + 2 * chunks;
-  uint32_t phase = 0;
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= chunks) break;
-    const int nw = (int)min((long long)CW, (n - c * CS) / 4);
-    if (nw == CW && a.has_map_in) {
-      if (tid == 0) {
-        fence_proxy_async();
-        mbar_expect_tx(&sm.bar, CS);
-        tma_load_rows(sm.buf0, &map_in, (int)(c * 128), &sm.bar);
-      }
-      if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
-      phase ^= 1;
-    } else {
-      load_plain_rows(sm.buf0, a.in, c, nw);
-      __syncthreads();
-    }
-    uint32_t v[32];
-    row_load(sm.buf0, tid, v);
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
-    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
-  }
-  finish_launch(a.sy);
+// ---- per-chunk bodies shared by the single-stream and batched kernels
+
+// Writes a stream header (int64 N, int32 exponent, int32 0).
+__device__ __forceinline__ void write_header(uint8_t* out, long long n, int eb_e) {
+  *reinterpret_cast<long long*>(out) = n;
+  reinterpret_cast<int*>(out)[2] = eb_e;
+  reinterpret_cast<int*>(out)[3] = 0;
 }
 
-// ---- init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel)
-template <int OP>
-__global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
-  Smem& sm = smem_block();
+// store (d_server_encode_kernel): one chunk of floats -> SQ -> encode.
+__device__ __forceinline__ void store_body(Smem& sm, const OpArgs& a, const CUtensorMap* map_in, long long c,
+                                           long long chunks, uint32_t& phase) {
   const int tid = threadIdx.x;
-  const StreamHdr h = read_header(a.in, a.in_bytes);
-  const bool hdr_ok = h.ok && h.n == a.n;
-  const long long chunks = hdr_ok ? h.chunks : 0;
-  if (tid == 0) {
-    mbar_init(&sm.bar, 1);
-    fence_mbar_init();
-    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+  const int nw = (int)min((long long)CW, (a.n - c * CS) / 4);
+  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
+  uint8_t* data = a.out + HDR + 2 * chunks;
+  if (nw == CW && a.has_map_in) {
+    if (tid == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&sm.bar, CS);
+      tma_load_rows(sm.buf0, map_in, (int)(c * 128), &sm.bar);
+    }
+    if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
+    phase ^= 1;
+  } else {
+    load_plain_rows(sm.buf0, a.in, c, nw);
+    __syncthreads();
   }
-  if (blockIdx.x == 0 && tid == 0) {
-    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
-    const long long n = hdr_ok ? h.n : 0;
-    *reinterpret_cast<long long*>(a.out) = n;
-    reinterpret_cast<int*>(a.out)[2] = (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e;
-    reinterpret_cast<int*>(a.out)[3] = 0;
-    if (chunks == 0) *a.out_size = HDR;
-  }
-  __syncthreads();
+  uint32_t v[32];
+  row_load(sm.buf0, tid, v);
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
+  if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+  else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
+}
+
+// init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
+// decode the stored chunk, requantize or form the residual, encode.
+template <int OP>
+__device__ __forceinline__ void reencode_body(Smem& sm, const OpArgs& a, const StreamHdr& h, DecState& ds, long long c) {
+  const int tid = threadIdx.x;
+  const long long chunks = h.chunks;
   const Quant qs = make_quant(h.eb_e);
   const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
   const uint8_t* din = a.in + HDR + 2 * chunks;
   const long long dbytes = a.in_bytes - HDR - 2 * chunks;
   uint16_t* tout = reinterpret_cast<uint16_t*>(a.out + HDR);
   uint8_t* dout = a.out + HDR + 2 * chunks;
-  DecState ds{0, 0, 0};
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= chunks) break;
-    const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
-    uint32_t v[32];
-    bool raw;
-    if (nw == CW) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
-    else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
-    // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
-    // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
+  const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
+  uint32_t v[32];
+  bool raw;
+  if (nw == CW) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
+  else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
+  // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
+  // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
 #pragma unroll
-    for (int k = 0; k < 32; k++) {
-      const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
-      if (OP == OP_S2C) {
-        v[k] = cq_enc(x, a.q1);
-      } else {
-        const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, a.q1), a.q1), a.q2);
-        v[k] = cq_enc(x, a.q2) - src_req;
-      }
+  for (int k = 0; k < 32; k++) {
+    const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+    if (OP == OP_S2C) {
+      v[k] = cq_enc(x, a.q1);
+    } else {
+      const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, a.q1), a.q1), a.q2);
+      v[k] = cq_enc(x, a.q2) - src_req;
     }
-    row_store(sm.buf0, tid, v);  // raw source: the bins / residuals
-    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
-    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
-    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
   }
-  finish_launch(a.sy);
+  row_store(sm.buf0, tid, v);  // raw source: the bins / residuals
+  if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
+  else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
 }
 
-// ---- storage decode / init_recv / resi_recv
+// storage decode / init_recv / resi_recv (d_server_decode_kernel,
+// d_client_decode_kernel, d_residual_apply_kernel).
 template <int OP>
-__global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
-                                               const __grid_constant__ CUtensorMap map_out) {
-  Smem& sm = smem_block();
+__device__ __forceinline__ void decode_body(Smem& sm, const OpArgs& a, const StreamHdr& h, DecState& ds, long long c,
+                                            const CUtensorMap* map_src, const CUtensorMap* map_out) {
   const int tid = threadIdx.x;
-  const StreamHdr h = read_header(a.in, a.in_bytes);
-  bool hdr_ok = h.ok && h.n <= a.out_cap;
-  if (OP == OP_RAPPLY) hdr_ok = hdr_ok && h.n == a.n;
-  const long long chunks = hdr_ok ? h.chunks : 0;
-  if (tid == 0) {
-    mbar_init(&sm.bar, 1);
-    fence_mbar_init();
-    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-  }
-  if (blockIdx.x == 0 && tid == 0) {
-    if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
-    *a.out_size = hdr_ok ? h.n : 0;
-  }
-  __syncthreads();
+  const long long chunks = h.chunks;
   const Quant q = make_quant(h.eb_e);
   const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
   const uint8_t* din = a.in + HDR + 2 * chunks;
   const long long dbytes = a.in_bytes - HDR - 2 * chunks;
   uint32_t* outbuf = (OP == OP_RAPPLY) ? sm_src(sm) : sm.buf0;
-  DecState ds{0, 0, 0};
+  const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
+  const bool full = nw == CW;
+  uint32_t v[32];
+  bool raw;
+  const bool tma_src = (OP == OP_RAPPLY) && full && a.has_map_in;
+  if (OP == OP_RAPPLY && !tma_src) load_plain_rows(sm_src(sm), a.src, c, nw);
+  if (full) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? map_src : nullptr, (int)(c * 128));
+  else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? map_src : nullptr, (int)(c * 128));
+  if (OP == OP_RAPPLY) {
+    // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
+    // destination bound, add the residual, dequantize.
+    uint32_t s2[32];
+    row_load(sm_src(sm), tid, s2);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s2[k], q) + v[k], q);
+  } else if (!raw) {
+    // chunks stored uncompressed are copied out as stored: original floats
+    // for storage decode (d_server_encode.h:234-249), request bins for
+    // init_recv (d_client_encode.h:230-254, the reference's behaviour)
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
+  }
+  row_store(outbuf, tid, v);
+  if (full && a.has_map_out) {
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_rows(map_out, (int)(c * 128), outbuf);
+      bulk_commit();
+    }
+  } else {
+    __syncthreads();
+    uint32_t* g = reinterpret_cast<uint32_t*>(a.out) + c * (long long)CW;
+    for (int w = tid; w < nw; w += NT) g[w] = outbuf[swz(w)];
+  }
+  if (OP == OP_RAPPLY && tid == 0) bulk_wait_read();  // buf2 is reloaded by the next chunk
+}
+
+__device__ __forceinline__ void launch_prologue(Smem& sm, const Sync& sy) {
+  begin_launch(sm, sy);
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+    sm.chunk = atomicAdd(&sy.counter[0], 1u);
+  }
+}
+
+// ---- single-stream kernels
+__global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
+  Smem& sm = smem_block();
+  const long long chunks = (a.n + CS - 1) / CS;
+  launch_prologue(sm, a.sy);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    write_header(a.out, a.n, a.q1.eb_e);
+    if (chunks == 0) *a.out_size = HDR;
+  }
+  __syncthreads();
+  uint32_t phase = 0;
   while (true) {
     const long long c = sm.chunk;
     if (c >= chunks) break;
-    const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
-    const bool full = nw == CW;
-    uint32_t v[32];
-    bool raw;
-    const bool tma_src = (OP == OP_RAPPLY) && full && a.has_map_in;
-    if (OP == OP_RAPPLY && !tma_src) load_plain_rows(sm_src(sm), a.src, c, nw);
-    if (full) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
-    else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? &map_src : nullptr, (int)(c * 128));
-    if (OP == OP_RAPPLY) {
-      // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
-      // destination bound, add the residual, dequantize.
-      uint32_t s[32];
-      row_load(sm_src(sm), tid, s);
-#pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s[k], q) + v[k], q);
-    } else if (!raw) {
-      // chunks stored uncompressed are copied out as stored: original floats
-      // for storage decode (d_server_encode.h:234-249), request bins for
-      // init_recv (d_client_encode.h:230-254, the reference's behaviour)
-#pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
-    }
-    row_store(outbuf, tid, v);
-    if (full && a.has_map_out) {
-      fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) {
-        tma_store_rows(&map_out, (int)(c * 128), outbuf);
-        bulk_commit();
-      }
-    } else {
-      __syncthreads();
-      uint32_t* g = reinterpret_cast<uint32_t*>(a.out) + c * (long long)CW;
-      for (int w = tid; w < nw; w += NT) g[w] = outbuf[swz(w)];
-    }
-    if (tid == 0) {
-      if (OP == OP_RAPPLY) bulk_wait_read();  // buf2 is reloaded by the next chunk
-      sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    }
+    store_body(sm, a, &map_in, c, chunks, phase);
+    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
     __syncthreads();
   }
-  if (tid == 0) bulk_wait_read();
-  finish_launch(a.sy);
+  finish_launch(sm, a.sy);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
+  Smem& sm = smem_block();
+  StreamHdr h = read_header(a.in, a.in_bytes);
+  const bool hdr_ok = h.ok && h.n == a.n;
+  if (!hdr_ok) h.chunks = 0;
+  launch_prologue(sm, a.sy);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
+    write_header(a.out, hdr_ok ? h.n : 0, (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e);
+    if (h.chunks == 0) *a.out_size = HDR;
+  }
+  __syncthreads();
+  DecState ds{0, 0, 0};
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= h.chunks) break;
+    reencode_body<OP>(sm, a, h, ds, c);
+    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    __syncthreads();
+  }
+  finish_launch(sm, a.sy);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
+                                               const __grid_constant__ CUtensorMap map_out) {
+  Smem& sm = smem_block();
+  StreamHdr h = read_header(a.in, a.in_bytes);
+  bool hdr_ok = h.ok && h.n <= a.out_cap;
+  if (OP == OP_RAPPLY) hdr_ok = hdr_ok && h.n == a.n;
+  if (!hdr_ok) h.chunks = 0;
+  launch_prologue(sm, a.sy);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
+    *a.out_size = hdr_ok ? h.n : 0;
+  }
+  __syncthreads();
+  DecState ds{0, 0, 0};
+  while (true) {
+    const long long c = sm.chunk;
+    if (c >= h.chunks) break;
+    decode_body<OP>(sm, a, h, ds, c, &map_src, &map_out);
+    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bulk_wait_read();
+  finish_launch(sm, a.sy);
+}
+
+// ---- batched kernels: one persistent launch over many streams.
+// The queue index runs over the items' chunks back to back; each item has its
+// own lookback words (Sync.flags offset by its chunk base), header and size.
+struct __align__(64) BatchItem {
+  CUtensorMap map_in;   // store: the floats; resi_recv: the client's floats
+  CUtensorMap map_out;  // decoders: the output floats
+  OpArgs a;             // a.sy.flags already offset to this item
+  long long chunk_base; // first queue index of this item
+  long long chunks;
+};
+
+// Item of queue index g (binary search over the items' chunk bases).
+__device__ __forceinline__ int find_item(const BatchItem* items, int n_items, long long g) {
+  int lo = 0, hi = n_items - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].chunk_base <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(NT, OP == OP_STORE ? MINB_STORE : (OP == OP_RAPPLY ? MINB_RAPPLY : (OP == OP_S2C || OP == OP_RESI) ? MINB_REENC : MINB_DEC))
+k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks, const __grid_constant__ Sync sy) {
+  Smem& sm = smem_block();
+  launch_prologue(sm, sy);
+  __syncthreads();
+  uint32_t phase = 0;
+  DecState ds{0, 0, 0};
+  int cur = -1;
+  while (true) {
+    const long long g = sm.chunk;
+    if (g >= total_chunks) break;
+    const int i = find_item(items, n_items, g);
+    const BatchItem& it = items[i];
+    const long long c = g - it.chunk_base;
+    if (i != cur) {  // a new stream: reset the decoders' running offset
+      cur = i;
+      ds.prev_c = 0;
+      ds.prev_off = 0;
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&it.map_in) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&it.map_out) : "memory");
+      }
+    }
+    if (OP == OP_STORE) {
+      if (c == 0 && threadIdx.x == 0) write_header(it.a.out, it.a.n, it.a.q1.eb_e);
+      store_body(sm, it.a, &it.map_in, c, it.chunks, phase);
+    } else {
+      StreamHdr h = read_header(it.a.in, it.a.in_bytes);
+      const bool ok = h.ok && h.n == it.a.n && (OP == OP_S2C || OP == OP_RESI || h.n <= it.a.out_cap);
+      if (!ok) {
+        if (threadIdx.x == 0) latch(sy.status, !h.ok ? DST_CORRUPT : DST_SIZE_MISMATCH);
+      } else if (OP == OP_S2C || OP == OP_RESI) {
+        if (c == 0 && threadIdx.x == 0) write_header(it.a.out, h.n, (OP == OP_S2C) ? it.a.q1.eb_e : it.a.q2.eb_e);
+        reencode_body<OP>(sm, it.a, h, ds, c);
+      } else {
+        if (c == 0 && threadIdx.x == 0) *it.a.out_size = h.n;
+        decode_body<OP>(sm, it.a, h, ds, c, &it.map_in, &it.map_out);
+      }
+    }
+    if (threadIdx.x == 0) sm.chunk = atomicAdd(&sy.counter[0], 1u);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bulk_wait_read();
+  finish_launch(sm, sy);
 }
 
 // ---- store without allocation (cortado_store_encode_noalloc)
 // Fixed scratch for callers that cannot allocate device memory: one
 // lookback word per chunk for up to CORTADO_NOALLOC_MAX_BYTES of input, then
-// the chunk queue, the finished-CTA count and the status word.  Every GPU that
+// the chunk queue, the finished-CTA count, the status word and the epoch.  Every GPU that
 // loads the library holds this array until the process exits.
 constexpr long long NOALLOC_CHUNKS = CORTADO_NOALLOC_MAX_BYTES / CS;
 __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_CHUNKS + 4];
 
 // Same chunk loop as k_store; the last CTA out also reports a device-side
 // error as a negative *out_size (there is no context to read it from) and
-// clears the status word for the next call.
+// clears the status word for the next call (finish_launch).
 __global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_constant__ OpArgs a,
                                                                   const __grid_constant__ CUtensorMap map_in) {
   Smem& sm = smem_block();
   const int tid = threadIdx.x;
   const long long n = a.n;
   const long long chunks = (n + CS - 1) / CS;
+  begin_launch(sm, a.sy);
   if (tid == 0) {
     mbar_init(&sm.bar, 1);
     fence_mbar_init();
@@ -314,15 +423,26 @@ __global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_c
     if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
     __syncthreads();
   }
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    if (atomicAdd(&a.sy.counter[1], 1u) == gridDim.x - 1) {
-      const unsigned int st = atomicExch(a.sy.status, 0u);
-      if (st) *a.out_size = -(long long)st;
-      a.sy.counter[0] = 0;
-      a.sy.counter[1] = 0;
-      __threadfence();
+  const unsigned int st = finish_launch(sm, a.sy, true);
+  if (st) *a.out_size = -(long long)st;
+}
+
+// ---- bound verifier (MAXABS_f32, include/verifiers/MAXABS_f32.h:40-72): the
+// first index whose reconstruction violates the absolute bound (NaN/Inf must
+// match: unequal unless both are NaN), or n if none.
+__device__ __forceinline__ bool maxabs_bad(float o, float r, float eb) {
+  if (!isfinite(o) || !isfinite(r)) return (r != o) && (!isnan(o) || !isnan(r));
+  const float lower = __fsub_rn(o, eb), upper = __fadd_rn(o, eb);
+  return (r < lower) || (r > upper) || (fabsf(__fsub_rn(o, r)) > eb);
+}
+
+__global__ void k_verify(const float* __restrict__ orig, const float* __restrict__ recon, long long nw, float eb,
+                         unsigned long long* first_bad) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += stride) {
+    if (maxabs_bad(orig[i], recon[i], eb)) {
+      atomicMin(first_bad, (unsigned long long)i);
+      return;
     }
   }
 }
@@ -365,8 +485,13 @@ struct cortado_ctx {
   int grid_store = 0, grid_reenc = 0, grid_dec = 0, grid_rapply = 0;
   unsigned long long* flags = nullptr;
   long long flags_cap = 0;
-  unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax
-  unsigned int epoch = 0;
+  unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax, [5] epoch
+  int grid_batch[6] = {0, 0, 0, 0, 0, 0};
+  int ctas_override[6] = {0, 0, 0, 0, 0, 0};  // per op: resident CTAs per SM (0 = occupancy limit)
+  BatchItem* d_items = nullptr;   // device item table of the batched launch
+  BatchItem* h_items = nullptr;   // pinned staging of the table
+  int items_cap = 0;
+  cudaEvent_t items_copied = nullptr;
   unsigned long long timeout_ns = 2000000000ull;
 };
 
@@ -433,20 +558,16 @@ cortado_status ensure_flags(cortado_ctx* ctx, int64_t chunks, cudaStream_t st) {
   e = cudaMemsetAsync(ctx->flags, 0, (size_t)cap * 8, st);
   if (e != cudaSuccess) return from_cuda(e);
   ctx->flags_cap = cap;
-  ctx->epoch = 0;
   return CORTADO_OK;
 }
 
-Sync next_sync(cortado_ctx* ctx, cudaStream_t st) {
-  if (++ctx->epoch >= 65536u) {
-    cudaMemsetAsync(ctx->flags, 0, (size_t)ctx->flags_cap * 8, st);
-    ctx->epoch = 1;
-  }
+Sync next_sync(cortado_ctx* ctx, cudaStream_t) {
   Sync s;
   s.flags = ctx->flags;
+  s.flags_cap = ctx->flags_cap;
   s.counter = ctx->words;
   s.status = ctx->words + 2;
-  s.epoch = ctx->epoch;
+  s.epoch = ctx->words + 5;
   s.timeout_ns = ctx->timeout_ns;
   return s;
 }
@@ -454,6 +575,15 @@ Sync next_sync(cortado_ctx* ctx, cudaStream_t st) {
 int grid_for(int per_sm_grid, int64_t chunks) {
   long long g = chunks < 1 ? 1 : chunks;
   return (int)(g < per_sm_grid ? g : per_sm_grid);
+}
+
+// Grid of an op: the tuned CTAs per SM if set (never above the occupancy
+// limit, which `occupancy` holds as a whole-GPU CTA count), else the limit.
+int tuned_grid(const cortado_ctx* ctx, int op, int occupancy) {
+  const int o = ctx->ctas_override[op];
+  if (o <= 0) return occupancy;
+  const long long g = (long long)o * ctx->sms;
+  return (int)(g < occupancy ? g : occupancy);
 }
 
 template <typename K>
@@ -523,6 +653,13 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
   occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_SRC, ctx->sms);
+  ctx->grid_batch[OP_STORE] = occupancy_grid(k_batch<OP_STORE>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_SRC, ctx->sms);
+  cudaEventCreateWithFlags(&ctx->items_copied, cudaEventDisableTiming);
   cortado_status s = ensure_flags(ctx, 1024, 0);
   cudaDeviceSynchronize();
   if (s != CORTADO_OK) { cortado_destroy(ctx); return s; }
@@ -536,12 +673,22 @@ void cortado_destroy(cortado_ctx* ctx) {
   cudaDeviceSynchronize();
   cudaFree(ctx->flags);
   cudaFree(ctx->words);
+  cudaFree(ctx->d_items);
+  cudaFreeHost(ctx->h_items);
+  if (ctx->items_copied) cudaEventDestroy(ctx->items_copied);
   delete ctx;
 }
 
 cortado_status cortado_set_timeout(cortado_ctx* ctx, uint64_t timeout_ns) {
   if (!ctx || timeout_ns == 0) return CORTADO_ERR_INVALID_ARG;
   ctx->timeout_ns = timeout_ns;
+  return CORTADO_OK;
+}
+
+cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas_per_sm) {
+  if (!ctx || op < CORTADO_OP_STORE || op > CORTADO_OP_RESI_RECV || ctas_per_sm < 0 || ctas_per_sm > 64)
+    return CORTADO_ERR_INVALID_ARG;
+  ctx->ctas_override[op] = ctas_per_sm;
   return CORTADO_OK;
 }
 
@@ -578,7 +725,7 @@ cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t 
   a.sy = next_sync(ctx, st);
   CUtensorMap map;
   a.has_map_in = make_rows_map(&map, d_in, n_bytes);
-  k_store<<<grid_for(ctx->grid_store, chunks), NT, SMEM_STD, st>>>(a, map);
+  k_store<<<grid_for(tuned_grid(ctx, OP_STORE, ctx->grid_store), chunks), NT, SMEM_STD, st>>>(a, map);
   return launch_status(cudaSuccess);
 }
 
@@ -606,7 +753,7 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.q1 = make_quant(e1);
   a.q2 = make_quant(e2);
   a.sy = next_sync(ctx, st);
-  const int grid = grid_for(ctx->grid_reenc, chunks);
+  const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
   if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
   else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
   return launch_status(cudaSuccess);
@@ -648,9 +795,9 @@ static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int
   a.has_map_out = make_rows_map(&mout, d_out, op == OP_RAPPLY ? n_bytes : out_capacity);
   if (op == OP_RAPPLY) a.has_map_in = make_rows_map(&msrc, d_src, n_bytes);
   const int64_t chunk_bound = chunks_of(op == OP_RAPPLY ? n_bytes : out_capacity);
-  if (op == OP_SDEC) k_decode<OP_SDEC><<<grid_for(ctx->grid_dec, chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
-  else if (op == OP_CDEC) k_decode<OP_CDEC><<<grid_for(ctx->grid_dec, chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
-  else k_decode<OP_RAPPLY><<<grid_for(ctx->grid_rapply, chunk_bound), NT, SMEM_SRC, st>>>(a, msrc, mout);
+  if (op == OP_SDEC) k_decode<OP_SDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
+  else if (op == OP_CDEC) k_decode<OP_CDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
+  else k_decode<OP_RAPPLY><<<grid_for(tuned_grid(ctx, op, ctx->grid_rapply), chunk_bound), NT, SMEM_SRC, st>>>(a, msrc, mout);
   return launch_status(cudaSuccess);
 }
 
@@ -670,6 +817,21 @@ cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_
   if (!d_src && n_bytes) return CORTADO_ERR_INVALID_ARG;
   if (n_bytes < 0 || (n_bytes & 3) || out_capacity < n_bytes) return n_bytes < 0 || (n_bytes & 3) ? CORTADO_ERR_INVALID_ARG : CORTADO_ERR_CAPACITY;
   return decode(ctx, OP_RAPPLY, d_resi, resi_bytes, d_src, n_bytes, d_out, out_capacity, d_outsize, stream);
+}
+
+cortado_status cortado_verify_bound(cortado_ctx* ctx, const void* d_orig, const void* d_recon, int64_t n_bytes,
+                                    float eb_abs, unsigned long long* d_first_bad, cortado_stream_t stream) {
+  if (!ctx || !d_orig || !d_recon || !d_first_bad || n_bytes < 0 || (n_bytes & 3) || !(eb_abs > 0))
+    return CORTADO_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long nw = n_bytes / 4;
+  cudaError_t e = cudaMemsetAsync(d_first_bad, 0xff, 8, st);
+  if (e != cudaSuccess) return from_cuda(e);
+  long long blocks = (nw + 255) / 256;
+  if (blocks > 8L * ctx->sms) blocks = 8L * ctx->sms;
+  if (blocks < 1) blocks = 1;
+  k_verify<<<(int)blocks, 256, 0, st>>>((const float*)d_orig, (const float*)d_recon, nw, eb_abs, d_first_bad);
+  return launch_status(cudaSuccess);
 }
 
 cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
@@ -698,13 +860,113 @@ cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_b
   return CORTADO_OK;
 }
 
+cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item* items, int n_items,
+                             cortado_stream_t stream) {
+  if (!ctx || !items || n_items <= 0 || op < CORTADO_OP_STORE || op > CORTADO_OP_RESI_RECV) return CORTADO_ERR_INVALID_ARG;
+  static_assert((int)CORTADO_OP_STORE == OP_STORE && (int)CORTADO_OP_INIT_SEND == OP_S2C &&
+                    (int)CORTADO_OP_RESI_SEND == OP_RESI && (int)CORTADO_OP_STORE_DECODE == OP_SDEC &&
+                    (int)CORTADO_OP_INIT_RECV == OP_CDEC && (int)CORTADO_OP_RESI_RECV == OP_RAPPLY,
+                "op numbering");
+  cudaStream_t st = (cudaStream_t)stream;
+  // per-item checks, as the single-stream entry points make them
+  long long total = 0;
+  for (int i = 0; i < n_items; i++) {
+    const cortado_item& it = items[i];
+    if (!it.d_in || !it.d_out || !it.d_outsize || it.n_bytes <= 0 || (it.n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
+    if (!aligned16(it.d_in) || !aligned16(it.d_out) || (it.d_src && !aligned16(it.d_src))) return CORTADO_ERR_ALIGNMENT;
+    int e = 0;
+    cortado_status s;
+    switch (op) {
+      case CORTADO_OP_STORE:
+        if (it.in_bytes != it.n_bytes) return CORTADO_ERR_INVALID_ARG;
+        if (it.out_capacity < cortado_max_stream_bytes(it.n_bytes)) return CORTADO_ERR_CAPACITY;
+        if ((s = eb_exponent(it.eb1 / 2, &e))) return s;
+        break;
+      case CORTADO_OP_INIT_SEND:
+      case CORTADO_OP_RESI_SEND:
+        if (it.in_bytes < HDR) return CORTADO_ERR_INVALID_ARG;
+        if (it.out_capacity < cortado_max_stream_bytes(it.n_bytes)) return CORTADO_ERR_CAPACITY;
+        if ((s = eb_exponent(it.eb1, &e))) return s;
+        if (op == CORTADO_OP_RESI_SEND && (s = eb_exponent(it.eb2, &e))) return s;
+        break;
+      case CORTADO_OP_RESI_RECV:
+        if (!it.d_src) return CORTADO_ERR_INVALID_ARG;
+        // fall through
+      default:
+        if (it.in_bytes < HDR) return CORTADO_ERR_INVALID_ARG;
+        if (it.out_capacity < it.n_bytes) return CORTADO_ERR_CAPACITY;
+        break;
+    }
+    total += chunks_of(it.n_bytes);
+  }
+  cortado_status s = ensure_flags(ctx, total, st);
+  if (s) return s;
+  if (n_items > ctx->items_cap) {
+    cudaStreamSynchronize(st);
+    cudaFree(ctx->d_items);
+    cudaFreeHost(ctx->h_items);
+    ctx->d_items = nullptr;
+    ctx->h_items = nullptr;
+    int cap = 64;
+    while (cap < n_items) cap *= 2;
+    cudaError_t e = cudaMalloc(&ctx->d_items, sizeof(BatchItem) * cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_items, sizeof(BatchItem) * cap);
+    if (e != cudaSuccess) { ctx->items_cap = 0; return from_cuda(e); }
+    ctx->items_cap = cap;
+  } else {
+    cudaEventSynchronize(ctx->items_copied);  // the staging table is free again
+  }
+  const Sync sy = next_sync(ctx, st);
+  long long base = 0;
+  for (int i = 0; i < n_items; i++) {
+    const cortado_item& it = items[i];
+    BatchItem& b = ctx->h_items[i];
+    memset(&b, 0, sizeof(b));
+    OpArgs& a = b.a;
+    a.in = (const uint8_t*)it.d_in;
+    a.in_bytes = it.in_bytes;
+    a.src = (const uint8_t*)it.d_src;
+    a.out = (uint8_t*)it.d_out;
+    a.out_cap = it.out_capacity;
+    a.out_size = (long long*)it.d_outsize;
+    a.n = it.n_bytes;
+    int e1 = 1, e2 = 1;
+    eb_exponent(op == CORTADO_OP_STORE ? it.eb1 / 2 : it.eb1, &e1);
+    eb_exponent(it.eb2, &e2);
+    a.q1 = make_quant(e1);
+    a.q2 = make_quant(e2);
+    a.sy = sy;
+    a.sy.flags = sy.flags + base;
+    if (op == CORTADO_OP_STORE) a.has_map_in = make_rows_map(&b.map_in, it.d_in, it.n_bytes);
+    if (op == CORTADO_OP_RESI_RECV) a.has_map_in = make_rows_map(&b.map_in, it.d_src, it.n_bytes);
+    if (op == CORTADO_OP_STORE_DECODE || op == CORTADO_OP_INIT_RECV || op == CORTADO_OP_RESI_RECV)
+      a.has_map_out = make_rows_map(&b.map_out, it.d_out, it.n_bytes);
+    b.chunk_base = base;
+    b.chunks = chunks_of(it.n_bytes);
+    base += b.chunks;
+  }
+  cudaError_t e = cudaMemcpyAsync(ctx->d_items, ctx->h_items, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return from_cuda(e);
+  cudaEventRecord(ctx->items_copied, st);
+  const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_batch[op]), total);
+  const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_SRC : SMEM_STD;
+  switch (op) {
+    case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_RESI_SEND: k_batch<OP_RESI><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_STORE_DECODE: k_batch<OP_SDEC><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_INIT_RECV: k_batch<OP_CDEC><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_RESI_RECV: k_batch<OP_RAPPLY><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+  }
+  return launch_status(cudaSuccess);
+}
+
 // Per-device set-up of the no-allocation entry point: the device address of
-// g_noalloc_scratch, the persistent grid size and the lookback epoch.
+// g_noalloc_scratch and the persistent grid size.
 struct NoallocDev {
   bool ready = false;
   unsigned long long* scratch = nullptr;
   int grid = 0;
-  unsigned int epoch = 0;
 };
 static NoallocDev g_noalloc_dev[64];
 static std::mutex g_noalloc_mu;
@@ -724,7 +986,6 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
   if (dev < 0 || dev >= 64) return CORTADO_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   NoallocDev& d = g_noalloc_dev[dev];
-  unsigned int epoch;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!d.ready) {
@@ -738,12 +999,6 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
       d.scratch = (unsigned long long*)p;
       d.ready = true;
     }
-    if (++d.epoch >= 65536u) {
-      ce = cudaMemsetAsync(d.scratch, 0, (size_t)NOALLOC_CHUNKS * 8, st);  // clears old lookback words
-      if (ce != cudaSuccess) return from_cuda(ce);
-      d.epoch = 1;
-    }
-    epoch = d.epoch;
   }
   OpArgs a{};
   a.in = (const uint8_t*)d_in;
@@ -754,9 +1009,10 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
   a.n = n_bytes;
   a.q1 = make_quant(e);
   a.sy.flags = d.scratch;
+  a.sy.flags_cap = NOALLOC_CHUNKS;
   a.sy.counter = reinterpret_cast<unsigned int*>(d.scratch + NOALLOC_CHUNKS);
   a.sy.status = a.sy.counter + 2;
-  a.sy.epoch = epoch;
+  a.sy.epoch = a.sy.counter + 3;
   a.sy.timeout_ns = 2000000000ull;
   CUtensorMap map;
   a.has_map_in = make_rows_map(&map, d_in, n_bytes);

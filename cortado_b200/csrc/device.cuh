@@ -49,11 +49,15 @@ __host__ __device__ inline Quant make_quant(int eb_e) {
 }
 
 // Per-launch bookkeeping shared by all CTAs (lives in the context workspace).
+// The launch epoch lives in device memory (read by every CTA at start,
+// advanced by the last CTA to finish), so launches captured in a CUDA graph
+// get a fresh epoch on every replay.
 struct Sync {
   unsigned long long* flags;  // lookback words, one per chunk (encoders)
+  long long flags_cap;        // words in flags (cleared when the epoch wraps)
   unsigned int* counter;      // [0] chunk queue, [1] CTAs finished
   unsigned int* status;       // first error latched
-  unsigned int epoch;         // 1..65535, tags this launch's lookback words
+  unsigned int* epoch;        // 0..65535, tags this launch's lookback words
   unsigned long long timeout_ns;
 };
 
@@ -295,12 +299,16 @@ constexpr unsigned long long LB_AGG = 1ull << 46, LB_INC = 2ull << 46, LB_VAL = 
 
 // Decoupled lookback over the chunk sizes (the role of propagate_carry,
 // include/d_compression.h:120-160).  Called by one whole warp; returns the
-// exclusive prefix of compressed bytes before chunk c.  Every wait is bounded:
-// on timeout, or when another CTA has already failed, the launch's status is
-// set and 0 is returned.
-__device__ __forceinline__ unsigned long long lookback(const Sync& sy, long long c, unsigned int csize) {
+// exclusive prefix of compressed bytes before chunk c.  Each poll reads the 32
+// nearest unaccounted predecessors (one per lane); once all have published,
+// the nearest inclusive prefix ends the walk, otherwise their sizes are added
+// and the window moves 32 chunks back.  Every wait is bounded: on timeout, or
+// when another CTA has already failed, the launch's status is set and 0 is
+// returned.
+__device__ __forceinline__ unsigned long long lookback(const Sync& sy, unsigned int epoch, long long c,
+                                                       unsigned int csize) {
   const int lane = threadIdx.x & 31;
-  const unsigned long long tag = (unsigned long long)sy.epoch << 48;
+  const unsigned long long tag = (unsigned long long)epoch << 48;
   if (lane == 0) st_relaxed(&sy.flags[c], tag | (c == 0 ? LB_INC : LB_AGG) | csize);
   if (c == 0) return 0;
   unsigned long long excl = 0;
@@ -309,11 +317,10 @@ __device__ __forceinline__ unsigned long long lookback(const Sync& sy, long long
   while (true) {
     const long long idx = top - lane;
     unsigned long long f = 0;
-    bool ready;
     int spins = 0;
     while (true) {
       f = (idx >= 0) ? ld_relaxed(&sy.flags[idx]) : (tag | LB_INC);
-      ready = ((f >> 48) == sy.epoch) && ((f & (3ull << 46)) != 0);
+      const bool ready = ((f >> 48) == epoch) && ((f & (3ull << 46)) != 0);
       if (__all_sync(0xffffffffu, ready)) break;
       if ((++spins & 31) == 0) {
         int bad = 0;

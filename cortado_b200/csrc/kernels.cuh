@@ -29,6 +29,7 @@ struct __align__(1024) Smem {
   uint64_t bar;
   long long chunk, next_chunk;
   unsigned long long payload_off;
+  unsigned int epoch, is_last;
   uint32_t info[8];
 };
 
@@ -114,7 +115,22 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
 
   // DIFFMS (d_DIFFMS.h:44-66): word minus its predecessor, then zig-zag.
   if (lane == 31) sm.xchg[warp] = v[31];
-  __syncthreads();
+  uint32_t vany = 0;
+#pragma unroll
+  for (int k = 0; k < 32; k++) vany |= v[k];
+  if (!__syncthreads_or(vany != 0)) {
+    // All words zero: DIFFMS, BIT_4 and zero elimination leave no byte, so
+    // RZE_1 emits only its 2-byte trailer (the original chunk size).
+    if (warp == 0) {
+      const unsigned long long X = lookback(a.sy, sm.epoch, c, 2u);
+      if (lane < 2) data_out[X + lane] = (uint8_t)(osize >> (8 * lane));
+      if (lane == 0) {
+        table_out[c] = 2;
+        if (c == chunks - 1) *a.out_size = HDR + 2 * chunks + (long long)(X + 2);
+      }
+    }
+    return;
+  }
   uint32_t prev = __shfl_up_sync(0xffffffffu, v[31], 1);
   if (lane == 0) prev = warp ? sm.xchg[warp - 1] : 0u;
 #pragma unroll
@@ -133,7 +149,10 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   // words s*G .. s*G+G-1); the trailing partial group is copied untransposed.
   uint32_t* plane = sm.buf1;
   if (FULL) {
-    transpose32(v);
+    uint32_t any = 0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) any |= v[k];
+    if (any) transpose32(v);  // an all-zero group transposes to all-zero planes
     uint32_t pe, po;
     plane_offsets(tid, pe, po);
 #pragma unroll
@@ -158,13 +177,18 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
       if (32 * tid + k >= nw) q[k] = 0;
   }
   // Zero-elimination bitmap (d_ZEencodebyteshort): bit i <-> byte i != 0.
-  uint32_t M[4];
+  uint32_t M[4] = {0, 0, 0, 0};
+  uint32_t qany = 0;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    uint32_t m = 0;
+  for (int k = 0; k < 32; k++) qany |= q[k];
+  if (qany) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) m |= nz_nibble(q[8 * j + i]) << (4 * i);
-    M[j] = m;
+    for (int j = 0; j < 4; j++) {
+      uint32_t m = 0;
+#pragma unroll
+      for (int i = 0; i < 8; i++) m |= nz_nibble(q[8 * j + i]) << (4 * i);
+      M[j] = m;
+    }
   }
   const uint32_t nz = __popc(M[0]) + __popc(M[1]) + __popc(M[2]) + __popc(M[3]);
   // Last bitmap byte of the previous segment (RE's predecessor of byte 0).
@@ -209,7 +233,7 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
     unsigned int csize = (NZ == 0) ? 2u : T + 6u;
     const bool raw = csize >= (unsigned)osize;
     if (raw) csize = osize;
-    const unsigned long long X = lookback(a.sy, c, csize);
+    const unsigned long long X = lookback(a.sy, sm.epoch, c, csize);
     if (lane == 0) {
       sm.info[0] = csize;
       sm.info[1] = raw;
@@ -301,10 +325,24 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   const int G = nw >> 5, rem = nw & 31;
   uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf0);
 
-  // Payload offset: warp 0 sums the size-table entries since its last chunk.
+  // Payload offset: warp 0 sums the size-table entries since its last chunk
+  // (8 entries per 16-byte load; the ragged ends entry by entry).
   if (warp == 0) {
     unsigned long long s = 0;
-    for (long long i = ds.prev_c + lane; i < c; i += 32) s += table[i];
+    const long long lo = ds.prev_c, hi = c;
+    const long long vlo = (lo + 7) & ~7LL, vhi = hi & ~7LL;  // 16-byte-aligned entries of the table
+    if (vlo < vhi) {
+      const uint4* t4 = reinterpret_cast<const uint4*>(table);
+      for (long long i = vlo / 8 + lane; i < vhi / 8; i += 32) {
+        const uint4 w = t4[i];
+        s += (w.x & 0xffffu) + (w.x >> 16) + (w.y & 0xffffu) + (w.y >> 16) + (w.z & 0xffffu) + (w.z >> 16) +
+             (w.w & 0xffffu) + (w.w >> 16);
+      }
+      for (long long i = lo + lane; i < vlo; i += 32) s += table[i];
+      for (long long i = vhi + lane; i < hi; i += 32) s += table[i];
+    } else {
+      for (long long i = lo + lane; i < hi; i += 32) s += table[i];
+    }
     s = warp_sum64(s);
     ds.prev_off += s;
     ds.prev_c = c;
@@ -375,6 +413,14 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   bool ok = true;
   const int orig = st[d + csize - 2] | (st[d + csize - 1] << 8);
   ok = (orig == osize);
+  if (csize == 2) {
+    // Trailer only: the BIT_4 output was all zero, so every word decodes to 0.
+    if (!ok && tid == 0) latch(a.sy.status, DST_CORRUPT);
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = 0;
+    __syncthreads();  // the trailer was read from buf0, which the caller reuses
+    return;
+  }
   uint32_t M[4] = {0, 0, 0, 0};
   uint32_t zbase = 0;
   if (csize == 2) {
@@ -456,11 +502,14 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   if (!ok) latch(a.sy.status, DST_CORRUPT);
   // ZE decode: scatter the non-zero bytes back into the 32 words.
   uint32_t q[32];
-  {
-    uint32_t p = (uint32_t)d + (ok ? zoff : 0u);
+  if (!ok || (M[0] | M[1] | M[2] | M[3]) == 0) {
+#pragma unroll
+    for (int k = 0; k < 32; k++) q[k] = 0;
+  } else {
+    uint32_t p = (uint32_t)d + zoff;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
-      const uint32_t m = ok ? (M[k >> 3] >> (4 * (k & 7))) & 15u : 0u;
+      const uint32_t m = (M[k >> 3] >> (4 * (k & 7))) & 15u;
       uint32_t x = 0;
       if (m) {
         const uint32_t lo = sm.buf0[p >> 2], hi = sm.buf0[(p >> 2) + 1];
@@ -476,9 +525,13 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   if (FULL) {
     uint32_t pe, po;
     plane_offsets(tid, pe, po);
+    uint32_t any = 0;
 #pragma unroll
-    for (int s = 0; s < 32; s++) v[s] = sm.buf1[128 * s + ((s & 1) ? po : pe)];
-    transpose32(v);
+    for (int s = 0; s < 32; s++) {
+      v[s] = sm.buf1[128 * s + ((s & 1) ? po : pe)];
+      any |= v[s];
+    }
+    if (any) transpose32(v);
   } else if (tid < G) {
 #pragma unroll
     for (int s = 0; s < 32; s++) v[s] = sm.buf1[swz(s * G + tid)];

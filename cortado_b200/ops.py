@@ -86,6 +86,10 @@ class Codec:
     def set_timeout(self, seconds: float):
         check(self._L.cortado_set_timeout(self._h, int(seconds * 1e9)), "set_timeout")
 
+    def set_launch_ctas(self, op: str, ctas_per_sm: int):
+        """Persistent-grid size of one operation (0 = occupancy limit)."""
+        check(self._L.cortado_set_launch_ctas(self._h, _native.OPS[op], int(ctas_per_sm)), "set_launch_ctas")
+
     def sync(self, stream=None):
         """Waits for the stream and raises the first device-detected error."""
         check(self._L.cortado_sync(self._h, _stream(stream)), "device")
@@ -127,6 +131,37 @@ class Codec:
         check(self._L.cortado_noa_range(self._h, _ptr(d_data), n, ctypes.byref(lo), ctypes.byref(hi),
                                         _stream(stream)), "INOA_find_range")
         return lo.value, hi.value
+
+    def verify_bound(self, orig, recon, eb_abs, first_bad=None, stream=None):
+        """MAXABS_f32 on the device: returns the int64 tensor holding the first
+        violating index (or -1 when every value is within eb_abs)."""
+        if first_bad is None:
+            first_bad = torch.empty(1, dtype=torch.int64, device=self.device)
+        check(self._L.cortado_verify_bound(self._h, _ptr(orig), _ptr(recon), _nbytes(orig), float(eb_abs),
+                                           _ptr(first_bad), _stream(stream)), "verify_bound")
+        return first_bad
+
+    # ------------------------------------------------ batched form
+    def batch(self, op: str, items, stream=None):
+        """Runs one operation on many streams in a single launch.
+
+        items: sequence of dicts with keys in (tensor), out (tensor), out_size
+        (int64 tensor slice), n_bytes, and as the operation needs eb1, eb2,
+        src (tensor), in_bytes (defaults to in's size)."""
+        arr = (_native.Item * len(items))()
+        for i, it in enumerate(items):
+            x = arr[i]
+            x.d_in = _ptr(it["in"])
+            x.in_bytes = int(it.get("in_bytes", _nbytes(it["in"])))
+            x.n_bytes = int(it["n_bytes"])
+            x.eb1 = float(it.get("eb1", 0.0))
+            x.eb2 = float(it.get("eb2", 0.0))
+            x.d_src = _ptr(it.get("src"))
+            x.d_out = _ptr(it["out"])
+            x.out_capacity = int(it.get("out_capacity", _nbytes(it["out"])))
+            x.d_outsize = _ptr(it["out_size"])
+        check(self._L.cortado_batch(self._h, _native.OPS[op], ctypes.cast(arr, ctypes.c_void_p), len(items),
+                                    _stream(stream)), "batch " + op)
 
     # ------------------------------------------------ convenience forms
     def _empty_stream(self, n_bytes):

@@ -118,6 +118,52 @@ cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_
 cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
                                  cortado_stream_t stream);
 
+/* Bound verifier: writes to *d_first_bad (device) the first index i at which
+ * recon[i] violates |orig[i] - recon[i]| <= eb_abs under the reference's
+ * MAXABS_f32 rules (include/verifiers/MAXABS_f32.h:40-72; NaN and Inf must
+ * match), or UINT64_MAX if every value is within the bound.  Asynchronous,
+ * so it can follow each step of a captured chain. */
+cortado_status cortado_verify_bound(cortado_ctx* ctx, const void* d_orig, const void* d_recon, int64_t n_bytes,
+                                    float eb_abs, unsigned long long* d_first_bad, cortado_stream_t stream);
+
+/* ---- batched form: many streams in one persistent launch ----
+ * No single counterpart in the reference (it launches one kernel per field
+ * and bound).  All items of one call run the same operation; their chunks
+ * form one work queue, so uneven sizes share the GPU without per-launch
+ * tails, and each item gets its own header, size table and offsets (a
+ * per-item lookback).  Every item needs its original size n_bytes (> 0). */
+typedef enum {
+  CORTADO_OP_STORE = 0,        /* d_in: floats (in_bytes == n_bytes), eb1: bound */
+  CORTADO_OP_INIT_SEND = 1,    /* d_in: stored stream, eb1: request bound */
+  CORTADO_OP_RESI_SEND = 2,    /* d_in: stored stream, eb1: source, eb2: destination bound */
+  CORTADO_OP_STORE_DECODE = 3, /* d_in: stored stream */
+  CORTADO_OP_INIT_RECV = 4,    /* d_in: init stream */
+  CORTADO_OP_RESI_RECV = 5     /* d_in: residual stream, d_src: the client's floats */
+} cortado_op;
+
+typedef struct {
+  const void* d_in;
+  int64_t in_bytes;
+  int64_t n_bytes;
+  float eb1, eb2;
+  const void* d_src;
+  void* d_out;
+  int64_t out_capacity;
+  int64_t* d_outsize;
+} cortado_item;
+
+/* Runs `op` on n_items items in one launch (replaces n_items calls of the
+ * corresponding entry point above, e.g. d_server_encode at 4 bounds for each
+ * of 64 fields).  Device-side errors are latched as for single calls. */
+cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item* items, int n_items,
+                             cortado_stream_t stream);
+
+/* Launch shape of `op` on this context: the persistent grid holds
+ * ctas_per_sm CTAs per SM (capped by the kernel's occupancy limit); 0 restores
+ * the occupancy limit.  Chosen by the autotuner (cortado_b200/autotune.py);
+ * it changes speed only, never output bytes. */
+cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas_per_sm);
+
 /* store without allocating: for callers that cannot call cudaMalloc.
  *
  * No counterpart in the reference.  Some callers of this library cannot
