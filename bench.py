@@ -278,6 +278,97 @@ def job_gbs(field_bytes: int, world: int, ms_per_step: float) -> float:
     return world * field_bytes * 1e-9 / (ms_per_step * 1e-3)
 
 
+def bench_batched(codec, dev, n_fields=64, seed=3, max_mb=256, bounds=("1e-1", "1e-2", "1e-3", "1e-4")):
+    """Many-fields configuration: n_fields float32 fields of log-uniform size
+    1 MiB .. max_mb MiB (multiples of 4 B, mixed generators), each stored at 4
+    NOA bounds -- one batched launch vs one launch per (field, bound)."""
+    from cortado_b200 import fields, storage
+    from cortado_b200.ops import max_stream_bytes
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kinds = ("sinusoid", "grf", "white")
+    xs = []
+    for i in range(n_fields):
+        nb = int(np.exp(rng.uniform(np.log(1 << 20), np.log(max_mb << 20)))) & ~3
+        xs.append(fields.mixed_field(nb // 4, kinds[i % 3], seed * 1000 + i, device=dev))
+    items, outs = [], []
+    sizes = torch.zeros(len(xs) * len(bounds), dtype=torch.int64, device=dev)
+    for i, x in enumerate(xs):
+        lo, hi = codec.INOA_find_range(x)
+        r = storage.value_range(lo, hi)
+        for j, b in enumerate(bounds):
+            k = i * len(bounds) + j
+            out = torch.empty(max_stream_bytes(x.numel() * 4), dtype=torch.uint8, device=dev)
+            outs.append(out)
+            items.append(dict(**{"in": x}, out=out, out_size=sizes[k:k + 1], n_bytes=x.numel() * 4,
+                              eb1=float(storage.noa_scale(b, r))))
+    total = sum(it["n_bytes"] for it in items)
+
+    def plain():
+        for it in items:
+            codec.server_encode(it["in"], it["n_bytes"], it["out"], it["out_size"], it["eb1"])
+
+    def batched():
+        codec.batch("store", items)
+
+    res = {}
+    for name, fn in (("plain", plain), ("batched", batched)):
+        fn()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ts = []
+        for _ in range(3):
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize(dev)
+            ts.append(s.elapsed_time(e))
+        res[name] = {"ms": float(np.median(ts)), "orig_GBps": total * 1e-9 / (np.median(ts) * 1e-3)}
+    codec.sync()
+    del outs
+    return {"workload": f"{n_fields} fields 1-{max_mb} MiB log-uniform (mixed sinusoid/GRF k^-3/white), "
+                        f"stored at NOA {list(bounds)}: {len(items)} encodes", "field_bytes_total": total // len(bounds),
+            **res, "speedup": res["plain"]["ms"] / res["batched"]["ms"]}
+
+
+def bench_serving(dev, n_fields=32, n_requests=400, rate_hz=2000.0, seed=5, max_mb=512):
+    """Serving configuration: resident stored fields (4..max_mb MiB, mixed
+    generators), Poisson arrivals (60% init at NOA 1e-1..1e-3, 40% residual 1-3
+    decades finer); continuous batching vs the plain per-request pipeline."""
+    from cortado_b200 import fields, storage
+    from cortado_b200.serve import Server, poisson_trace
+    rng = np.random.Generator(np.random.PCG64(seed))
+    srv = Server(dev.index, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3)
+    kinds = ("sinusoid", "grf", "white")
+    ranges = {}
+    for i in range(n_fields):
+        nb = int(np.exp(rng.uniform(np.log(4 << 20), np.log(max_mb << 20)))) & ~3
+        x = fields.mixed_field(nb // 4, kinds[i % 3], seed * 1000 + i, device=dev)
+        r = float(x.max() - x.min())
+        ranges[f"f{i}"] = r
+        srv.add_field(f"f{i}", x, [float(storage.noa_scale(e, r)) for e in (1e-1, 1e-3, 1e-5, 1e-7)])
+    trace = poisson_trace(rng, srv.fields, n_requests, rate_hz, n_clients=16, ranges=ranges)
+    # Client reconstructions are allocated up front (a server does that when a
+    # client opens a field); each mode serves the trace once untimed, so the
+    # allocator holds its output streams, then once measured, from fresh
+    # client progress on the same buffers.
+    srv.prepare(trace)
+
+    def once(fn):
+        srv.reset_clients(free=False)
+        for r in trace:
+            r.done = -1.0
+        return fn(trace)[0]
+
+    once(srv.run)
+    served = once(srv.run)
+    once(srv.run_plain)
+    plain = once(srv.run_plain)
+    srv.close()
+    return {"workload": f"{n_fields} resident fields 4-{max_mb} MiB, {n_requests} requests, Poisson {rate_hz:g}/s, "
+                        "60% init / 40% residual", "served": served, "plain": plain,
+            "speedup": served["orig_GBps"] / plain["orig_GBps"] if plain["orig_GBps"] else None}
+
+
 def load_traffic():
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
@@ -315,6 +406,7 @@ def main():
     ap.add_argument("--cpu-sample-mb", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="512,512,512", help="field shape (profiling uses a smaller one)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     args = ap.parse_args()
     args.shape = tuple(int(v) for v in args.shape.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -386,6 +478,15 @@ def main():
                              for k, t in zip(OPS, r["abs"]["per_op"])}},
         "clocks": r["clocks"],
     }
+    if not args.no_extras and world == 1:
+        from cortado_b200.ops import Codec
+        dev = torch.device("cuda", 0)
+        c = Codec(0)
+        line["batched"] = bench_batched(c, dev)
+        c.close()
+        torch.cuda.empty_cache()
+        line["serving"] = bench_serving(dev)
+        torch.cuda.empty_cache()
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_sample_mb)
     print(json.dumps(line))

@@ -488,10 +488,16 @@ struct cortado_ctx {
   unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax, [5] epoch
   int grid_batch[6] = {0, 0, 0, 0, 0, 0};
   int ctas_override[6] = {0, 0, 0, 0, 0, 0};  // per op: resident CTAs per SM (0 = occupancy limit)
-  BatchItem* d_items = nullptr;   // device item table of the batched launch
-  BatchItem* h_items = nullptr;   // pinned staging of the table
+  // Item tables of the batched launch: a ring of ITEM_SLOTS slots, each with
+  // items_cap entries in pinned host staging and in device memory, and an
+  // event recorded after the launch that read it.  A call waits only for the
+  // launch ITEM_SLOTS calls back, so the host keeps running ahead of the GPU.
+  static constexpr int ITEM_SLOTS = 8;
+  BatchItem* d_items = nullptr;
+  BatchItem* h_items = nullptr;
   int items_cap = 0;
-  cudaEvent_t items_copied = nullptr;
+  int items_slot = 0;
+  cudaEvent_t items_done[ITEM_SLOTS] = {};
   unsigned long long timeout_ns = 2000000000ull;
 };
 
@@ -659,7 +665,7 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_SRC, ctx->sms);
-  cudaEventCreateWithFlags(&ctx->items_copied, cudaEventDisableTiming);
+  for (cudaEvent_t& ev : ctx->items_done) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   cortado_status s = ensure_flags(ctx, 1024, 0);
   cudaDeviceSynchronize();
   if (s != CORTADO_OK) { cortado_destroy(ctx); return s; }
@@ -675,7 +681,8 @@ void cortado_destroy(cortado_ctx* ctx) {
   cudaFree(ctx->words);
   cudaFree(ctx->d_items);
   cudaFreeHost(ctx->h_items);
-  if (ctx->items_copied) cudaEventDestroy(ctx->items_copied);
+  for (cudaEvent_t ev : ctx->items_done)
+    if (ev) cudaEventDestroy(ev);
   delete ctx;
 }
 
@@ -901,26 +908,30 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   }
   cortado_status s = ensure_flags(ctx, total, st);
   if (s) return s;
+  constexpr int SLOTS = cortado_ctx::ITEM_SLOTS;
   if (n_items > ctx->items_cap) {
-    cudaStreamSynchronize(st);
+    for (cudaEvent_t ev : ctx->items_done) cudaEventSynchronize(ev);  // every table is free
     cudaFree(ctx->d_items);
     cudaFreeHost(ctx->h_items);
     ctx->d_items = nullptr;
     ctx->h_items = nullptr;
     int cap = 64;
     while (cap < n_items) cap *= 2;
-    cudaError_t e = cudaMalloc(&ctx->d_items, sizeof(BatchItem) * cap);
-    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_items, sizeof(BatchItem) * cap);
+    cudaError_t e = cudaMalloc(&ctx->d_items, sizeof(BatchItem) * cap * SLOTS);
+    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_items, sizeof(BatchItem) * cap * SLOTS);
     if (e != cudaSuccess) { ctx->items_cap = 0; return from_cuda(e); }
     ctx->items_cap = cap;
-  } else {
-    cudaEventSynchronize(ctx->items_copied);  // the staging table is free again
   }
+  const int slot = ctx->items_slot;
+  ctx->items_slot = (slot + 1) % SLOTS;
+  cudaEventSynchronize(ctx->items_done[slot]);  // the launch that last read this slot has ended
+  BatchItem* h_tab = ctx->h_items + (size_t)slot * ctx->items_cap;
+  BatchItem* d_tab = ctx->d_items + (size_t)slot * ctx->items_cap;
   const Sync sy = next_sync(ctx, st);
   long long base = 0;
   for (int i = 0; i < n_items; i++) {
     const cortado_item& it = items[i];
-    BatchItem& b = ctx->h_items[i];
+    BatchItem& b = h_tab[i];
     memset(&b, 0, sizeof(b));
     OpArgs& a = b.a;
     a.in = (const uint8_t*)it.d_in;
@@ -945,19 +956,19 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
     b.chunks = chunks_of(it.n_bytes);
     base += b.chunks;
   }
-  cudaError_t e = cudaMemcpyAsync(ctx->d_items, ctx->h_items, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(d_tab, h_tab, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return from_cuda(e);
-  cudaEventRecord(ctx->items_copied, st);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_batch[op]), total);
   const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_SRC : SMEM_STD;
   switch (op) {
-    case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
-    case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
-    case CORTADO_OP_RESI_SEND: k_batch<OP_RESI><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
-    case CORTADO_OP_STORE_DECODE: k_batch<OP_SDEC><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
-    case CORTADO_OP_INIT_RECV: k_batch<OP_CDEC><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
-    case CORTADO_OP_RESI_RECV: k_batch<OP_RAPPLY><<<grid, NT, smem, st>>>(ctx->d_items, n_items, total, sy); break;
+    case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_RESI_SEND: k_batch<OP_RESI><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_STORE_DECODE: k_batch<OP_SDEC><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_INIT_RECV: k_batch<OP_CDEC><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_RESI_RECV: k_batch<OP_RAPPLY><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
   }
+  cudaEventRecord(ctx->items_done[slot], st);
   return launch_status(cudaSuccess);
 }
 

@@ -304,12 +304,12 @@ constexpr unsigned long long LB_AGG = 1ull << 46, LB_INC = 2ull << 46, LB_VAL = 
 // the nearest inclusive prefix ends the walk, otherwise their sizes are added
 // and the window moves 32 chunks back.  Every wait is bounded: on timeout, or
 // when another CTA has already failed, the launch's status is set and 0 is
-// returned.
-__device__ __forceinline__ unsigned long long lookback(const Sync& sy, unsigned int epoch, long long c,
-                                                       unsigned int csize) {
+// returned.  lookback_published expects chunk c's own word to be published
+// already (lookback_publish), so a caller can do other work in between.
+__device__ __forceinline__ unsigned long long lookback_published(const Sync& sy, unsigned int epoch, long long c,
+                                                                 unsigned int csize) {
   const int lane = threadIdx.x & 31;
   const unsigned long long tag = (unsigned long long)epoch << 48;
-  if (lane == 0) st_relaxed(&sy.flags[c], tag | (c == 0 ? LB_INC : LB_AGG) | csize);
   if (c == 0) return 0;
   unsigned long long excl = 0;
   long long top = c - 1;
@@ -343,6 +343,19 @@ __device__ __forceinline__ unsigned long long lookback(const Sync& sy, unsigned 
   }
   if (lane == 0) st_relaxed(&sy.flags[c], tag | LB_INC | (excl + csize));
   return excl;
+}
+
+// Publishes chunk c's own size (one thread): the inclusive prefix for chunk 0,
+// the aggregate otherwise.
+__device__ __forceinline__ void lookback_publish(const Sync& sy, unsigned int epoch, long long c,
+                                                 unsigned int csize) {
+  st_relaxed(&sy.flags[c], ((unsigned long long)epoch << 48) | (c == 0 ? LB_INC : LB_AGG) | csize);
+}
+
+__device__ __forceinline__ unsigned long long lookback(const Sync& sy, unsigned int epoch, long long c,
+                                                       unsigned int csize) {
+  if ((threadIdx.x & 31) == 0) lookback_publish(sy, epoch, c, csize);
+  return lookback_published(sy, epoch, c, csize);
 }
 
 }  // namespace cortado

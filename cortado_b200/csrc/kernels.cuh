@@ -216,6 +216,7 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   // (barrier inside the scan: the plane buffer is now free -> staging)
   uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf1);
 
+  unsigned int w0_csize = 0;
   if (warp == 0) {
     // Levels 2 and 3 and the top bitmap (d_REencode1wordperthread), one warp.
     const uint2 b2 = reinterpret_cast<const uint2*>(sm.l2)[lane];
@@ -233,12 +234,13 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
     unsigned int csize = (NZ == 0) ? 2u : T + 6u;
     const bool raw = csize >= (unsigned)osize;
     if (raw) csize = osize;
-    const unsigned long long X = lookback(a.sy, sm.epoch, c, csize);
+    // Publish now, wait for the predecessors' prefix after the compaction.
     if (lane == 0) {
+      lookback_publish(a.sy, sm.epoch, c, csize);
       sm.info[0] = csize;
       sm.info[1] = raw;
-      sm.payload_off = X;
     }
+    w0_csize = csize;
     if (!raw) {
       if (NZ == 0) {
         if (lane == 0) {
@@ -285,6 +287,10 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
 #pragma unroll
     for (int j = 0; j < 16; j++)
       if ((K >> j) & 1) st[p++] = (uint8_t)(M[j >> 2] >> (8 * (j & 3)));
+  }
+  if (warp == 0) {
+    const unsigned long long X = lookback_published(a.sy, sm.epoch, c, w0_csize);
+    if (lane == 0) sm.payload_off = X;
   }
   __syncthreads();
   const unsigned int csize = sm.info[0];

@@ -105,13 +105,18 @@ class Server:
         codec, s = self.codecs[k], self.streams[k]
         inits = [r for r in reqs if r.kind == "init"]
         resis = [r for r in reqs if r.kind == "resi"]
-        outs, sizes = {}, torch.zeros(max(1, len(reqs)) * 2, dtype=torch.int64, device=self.dev)
+        # Everything this batch allocates is allocated on its own stream, so the
+        # caching allocator orders the memory with the batch's launches.
+        with torch.cuda.stream(s):
+            sizes = torch.empty(max(1, len(reqs)) * 2, dtype=torch.int64, device=self.dev)
+        outs = {}
         j = 0
         items_send, items_recv = [], []
         for r in inits:
             f = self.fields[r.field]
             st = self._recon(r.client, r.field)
-            out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
+            with torch.cuda.stream(s):
+                out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
                                    n_bytes=f.n_bytes, eb1=r.bound))
@@ -128,7 +133,8 @@ class Server:
             st = self._recon(r.client, r.field)
             if st["bound"] is None:
                 raise ValueError(f"request {r.rid}: residual before init")
-            out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
+            with torch.cuda.stream(s):
+                out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
                                    n_bytes=f.n_bytes, eb1=st["bound"], eb2=r.bound))
@@ -162,16 +168,13 @@ class Server:
                 ev, reqs, outs, sizes, nbytes, _ = item
                 if ev.query():
                     tdone = time.perf_counter() - t0
-                    sz = sizes.cpu().tolist()
-                    for jj, r in enumerate(reqs):
+                    for r in reqs:
                         r.done = tdone
                         busy_clients.discard((r.client, r.field))
                     if keep_outputs:
                         for r in reqs:
                             outputs[r.rid] = outs[r.rid]
                     self.mem_used -= nbytes
-                    for c in self.codecs:
-                        pass
                 else:
                     still.append(item)
             inflight = still
@@ -206,10 +209,14 @@ class Server:
 
     def run_plain(self, requests: list[Request], keep_outputs=False):
         """The plain per-request pipeline: requests in arrival order, each as
-        its own init_send/init_recv or resi_send/resi_recv calls, synchronized."""
+        its own send and receive call (the reference-shaped single-stream entry
+        points, decoding straight into the client's reconstruction),
+        synchronized after every request."""
         pending = sorted(requests, key=lambda r: r.arrival)
         codec, s = self.codecs[0], self.streams[0]
         outputs = {}
+        with torch.cuda.stream(s):
+            sizes = torch.empty(2, dtype=torch.int64, device=self.dev)
         t0 = time.perf_counter()
         for r in pending:
             now = time.perf_counter() - t0
@@ -217,15 +224,17 @@ class Server:
                 time.sleep(r.arrival - now)
             f = self.fields[r.field]
             st = self._recon(r.client, r.field)
+            stored = self._stored_for(f, r.bound)
             with torch.cuda.stream(s):
+                out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
                 if r.kind == "init":
-                    out = codec.init_send(self._stored_for(f, r.bound), r.bound, n_bytes=f.n_bytes)
-                    st["recon"].copy_(codec.init_recv(out, n_bytes=f.n_bytes))
+                    codec.s2c_encode(stored, out, sizes[0:1], r.bound, f.n_bytes, stream=s)
+                    codec.client_decode(out, st["recon"], sizes[1:2], stream=s)
                 else:
-                    out = codec.resi_send(self._stored_for(f, r.bound), st["bound"], r.bound, n_bytes=f.n_bytes)
-                    st["recon"].copy_(codec.resi_recv(st["recon"], out))
+                    codec.residual_encode(stored, out, sizes[0:1], st["bound"], r.bound, f.n_bytes, stream=s)
+                    codec.residual_apply(st["recon"], f.n_bytes, out, st["recon"], sizes[1:2], stream=s)
                 st["bound"] = r.bound
-            torch.cuda.synchronize(self.dev)
+            codec.sync(s)
             r.done = time.perf_counter() - t0
             if keep_outputs:
                 outputs[r.rid] = out
@@ -239,7 +248,20 @@ class Server:
                 "p50_ms": float(np.percentile(lat, 50) * 1e3) if lat.size else None,
                 "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else None}
 
-    def reset_clients(self):
+    def prepare(self, requests: list[Request]):
+        """Allocates the reconstruction of every (client, field) the requests
+        touch, as a server does when a client opens a field, so that serving
+        itself allocates only output streams."""
+        for r in requests:
+            self._recon(r.client, r.field)
+        torch.cuda.synchronize(self.dev)
+
+    def reset_clients(self, free=True):
+        """Forgets every client's progress; free=False keeps the buffers."""
+        if not free:
+            for st in self.clients.values():
+                st["bound"] = None
+            return
         for (c, fname), st in self.clients.items():
             self.mem_used -= self.fields[fname].n_bytes
         self.clients.clear()
