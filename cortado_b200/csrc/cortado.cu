@@ -17,13 +17,13 @@ using namespace cortado;
 
 // ================================================================== kernels
 // Resident CTAs per SM each kernel is compiled for (register budget
-// 65536 / (128 * n)).  resi_recv holds a third 16 KiB buffer, so shared memory
-// limits it to 4.
+// 65536 / (128 * n)).  init_send, resi_send and resi_recv hold a third 17 KiB
+// buffer, so shared memory limits them to 4.
 #ifndef MINB_STORE
 #define MINB_STORE 6
 #endif
 #ifndef MINB_REENC
-#define MINB_REENC 5
+#define MINB_REENC 4
 #endif
 #ifndef MINB_DEC
 #define MINB_DEC 6
@@ -34,21 +34,36 @@ using namespace cortado;
 
 namespace {
 
-__device__ __forceinline__ Smem& smem_block() {
+__device__ __forceinline__ Ctl& ctl_block() {
   extern __shared__ uint8_t smem_raw[];
-  return *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  return *reinterpret_cast<Ctl*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 }
 
-// Reads this launch's lookback epoch (every CTA, at start).
-__device__ __forceinline__ void begin_launch(Smem& sm, const Sync& sy) {
+// The thread that issues every TMA load and store of a CTA (warp 3, lane 0):
+// bulk-store completion is tracked per thread, so the thread that reuses a
+// buffer after a TMA store must be the one that issued the store.
+constexpr int TMA_TID = 96;
+
+// Reads this launch's lookback epoch and sets up the stage barriers (every
+// CTA, at start; the caller synchronizes).  A stage's barrier completes a
+// phase per use: two arrivals by the prefetching lane (one before its loads
+// are issued, one after the stage's metadata and hand-copied bytes are
+// written) plus the TMA bytes, so waiting on it also publishes the metadata.
+__device__ __forceinline__ void begin_launch(Ctl& sm, const Sync& sy) {
   if (threadIdx.x == 0) sm.epoch = *(volatile unsigned int*)sy.epoch;
+  if (threadIdx.x == TMA_TID) {
+    mbar_init(&sm.bar[0], 2);
+    mbar_init(&sm.bar[1], 2);
+    mbar_init(&sm.bar_src, 1);
+    fence_mbar_init();
+  }
 }
 
 // The last CTA out resets the chunk queue and advances the epoch for the next
 // launch on this scratch; when the 16-bit epoch wraps it first clears the
 // lookback words, so no word of an old launch can carry the new epoch.
 // Returns the status word's value to the last CTA's thread 0 (else 0).
-__device__ __forceinline__ unsigned int finish_launch(Smem& sm, const Sync& sy, bool take_status = false) {
+__device__ __forceinline__ unsigned int finish_launch(Ctl& sm, const Sync& sy, bool take_status = false) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -59,7 +74,10 @@ __device__ __forceinline__ unsigned int finish_launch(Smem& sm, const Sync& sy, 
   if (sm.is_last) {
     const unsigned int e = sm.epoch;
     if (e == 65535u)
-      for (long long i = threadIdx.x; i < sy.flags_cap; i += blockDim.x) sy.flags[i] = 0;
+      for (long long i = threadIdx.x; i < sy.flags_cap; i += blockDim.x) {
+        sy.flags[i] = 0;
+        if (sy.offs) sy.offs[i] = 0;
+      }
     __syncthreads();
     if (threadIdx.x == 0) {
       if (take_status) st = atomicExch(sy.status, 0u);
@@ -72,7 +90,7 @@ __device__ __forceinline__ unsigned int finish_launch(Smem& sm, const Sync& sy, 
   return st;
 }
 
-// Loads the full-chunk float words of group g from a swizzled buffer.
+// Loads the float words of a chunk into a swizzled buffer (zero past nw).
 __device__ __forceinline__ void load_plain_rows(uint32_t* buf, const uint8_t* src, long long c, int nw) {
   const uint32_t* g = reinterpret_cast<const uint32_t*>(src) + c * (long long)CW;
   for (int w = threadIdx.x; w < CW; w += NT) buf[swz(w)] = (w < nw) ? g[w] : 0u;
@@ -96,8 +114,6 @@ __device__ __forceinline__ StreamHdr read_header(const uint8_t* s, long long byt
   return h;
 }
 
-// ---- per-chunk bodies shared by the single-stream and batched kernels
-
 // Writes a stream header (int64 N, int32 exponent, int32 0).
 __device__ __forceinline__ void write_header(uint8_t* out, long long n, int eb_e) {
   *reinterpret_cast<long long*>(out) = n;
@@ -105,200 +121,34 @@ __device__ __forceinline__ void write_header(uint8_t* out, long long n, int eb_e
   reinterpret_cast<int*>(out)[3] = 0;
 }
 
-// store (d_server_encode_kernel): one chunk of floats -> SQ -> encode.
-__device__ __forceinline__ void store_body(Smem& sm, const OpArgs& a, const CUtensorMap* map_in, long long c,
-                                           long long chunks, uint32_t& phase) {
-  const int tid = threadIdx.x;
-  const int nw = (int)min((long long)CW, (a.n - c * CS) / 4);
-  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
-  uint8_t* data = a.out + HDR + 2 * chunks;
-  if (nw == CW && a.has_map_in) {
-    if (tid == 0) {
-      fence_proxy_async();
-      mbar_expect_tx(&sm.bar, CS);
-      tma_load_rows(sm.buf0, map_in, (int)(c * 128), &sm.bar);
-    }
-    if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
-    phase ^= 1;
-  } else {
-    load_plain_rows(sm.buf0, a.in, c, nw);
-    __syncthreads();
+// ---- work sources: what a queue index means.
+// One stream: the queue index is the chunk; arguments and tensor maps are the
+// kernel's own parameters; a decoder's header was checked at kernel start.
+struct SingleSrc {
+  static constexpr bool batched = false;
+  const OpArgs* a;
+  const CUtensorMap* map_in;
+  const CUtensorMap* map_out;
+  long long total;
+  StreamHdr h;
+  __device__ __forceinline__ int locate(long long g, int, long long& c) const {
+    c = g;
+    return 0;
   }
-  uint32_t v[32];
-  row_load(sm.buf0, tid, v);
-#pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
-  if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-  else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-}
+  __device__ __forceinline__ const OpArgs& args(int) const { return *a; }
+  __device__ __forceinline__ const CUtensorMap* min(int) const { return map_in; }
+  __device__ __forceinline__ const CUtensorMap* mout(int) const { return map_out; }
+  __device__ __forceinline__ StreamHdr header(int) const { return h; }
+  __device__ __forceinline__ int header_bad(int, const StreamHdr&) const { return 0; }
+  // offset scanner over the stream's size table (one warp)
+  __device__ __forceinline__ void scan(unsigned int epoch) const {
+    if (total > 0) scan_offsets(a->sy.offs, epoch, reinterpret_cast<const uint16_t*>(a->in + HDR), h.chunks);
+  }
+};
 
-// init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
-// decode the stored chunk, requantize or form the residual, encode.
-template <int OP>
-__device__ __forceinline__ void reencode_body(Smem& sm, const OpArgs& a, const StreamHdr& h, DecState& ds, long long c) {
-  const int tid = threadIdx.x;
-  const long long chunks = h.chunks;
-  const Quant qs = make_quant(h.eb_e);
-  const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
-  const uint8_t* din = a.in + HDR + 2 * chunks;
-  const long long dbytes = a.in_bytes - HDR - 2 * chunks;
-  uint16_t* tout = reinterpret_cast<uint16_t*>(a.out + HDR);
-  uint8_t* dout = a.out + HDR + 2 * chunks;
-  const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
-  uint32_t v[32];
-  bool raw;
-  if (nw == CW) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
-  else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, nullptr, 0);
-  // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
-  // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
-#pragma unroll
-  for (int k = 0; k < 32; k++) {
-    const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
-    if (OP == OP_S2C) {
-      v[k] = cq_enc(x, a.q1);
-    } else {
-      const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, a.q1), a.q1), a.q2);
-      v[k] = cq_enc(x, a.q2) - src_req;
-    }
-  }
-  row_store(sm.buf0, tid, v);  // raw source: the bins / residuals
-  if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
-  else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, dout, tout);
-}
-
-// storage decode / init_recv / resi_recv (d_server_decode_kernel,
-// d_client_decode_kernel, d_residual_apply_kernel).
-template <int OP>
-__device__ __forceinline__ void decode_body(Smem& sm, const OpArgs& a, const StreamHdr& h, DecState& ds, long long c,
-                                            const CUtensorMap* map_src, const CUtensorMap* map_out) {
-  const int tid = threadIdx.x;
-  const long long chunks = h.chunks;
-  const Quant q = make_quant(h.eb_e);
-  const uint16_t* tin = reinterpret_cast<const uint16_t*>(a.in + HDR);
-  const uint8_t* din = a.in + HDR + 2 * chunks;
-  const long long dbytes = a.in_bytes - HDR - 2 * chunks;
-  uint32_t* outbuf = (OP == OP_RAPPLY) ? sm_src(sm) : sm.buf0;
-  const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
-  const bool full = nw == CW;
-  uint32_t v[32];
-  bool raw;
-  const bool tma_src = (OP == OP_RAPPLY) && full && a.has_map_in;
-  if (OP == OP_RAPPLY && !tma_src) load_plain_rows(sm_src(sm), a.src, c, nw);
-  if (full) decode_chunk<true>(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? map_src : nullptr, (int)(c * 128));
-  else decode_chunk_partial(sm, a, ds, c, nw, chunks, tin, din, dbytes, v, raw, tma_src ? map_src : nullptr, (int)(c * 128));
-  if (OP == OP_RAPPLY) {
-    // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
-    // destination bound, add the residual, dequantize.
-    uint32_t s2[32];
-    row_load(sm_src(sm), tid, s2);
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s2[k], q) + v[k], q);
-  } else if (!raw) {
-    // chunks stored uncompressed are copied out as stored: original floats
-    // for storage decode (d_server_encode.h:234-249), request bins for
-    // init_recv (d_client_encode.h:230-254, the reference's behaviour)
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
-  }
-  row_store(outbuf, tid, v);
-  if (full && a.has_map_out) {
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      tma_store_rows(map_out, (int)(c * 128), outbuf);
-      bulk_commit();
-    }
-  } else {
-    __syncthreads();
-    uint32_t* g = reinterpret_cast<uint32_t*>(a.out) + c * (long long)CW;
-    for (int w = tid; w < nw; w += NT) g[w] = outbuf[swz(w)];
-  }
-  if (OP == OP_RAPPLY && tid == 0) bulk_wait_read();  // buf2 is reloaded by the next chunk
-}
-
-__device__ __forceinline__ void launch_prologue(Smem& sm, const Sync& sy) {
-  begin_launch(sm, sy);
-  if (threadIdx.x == 0) {
-    mbar_init(&sm.bar, 1);
-    fence_mbar_init();
-    sm.chunk = atomicAdd(&sy.counter[0], 1u);
-  }
-}
-
-// ---- single-stream kernels
-__global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
-  Smem& sm = smem_block();
-  const long long chunks = (a.n + CS - 1) / CS;
-  launch_prologue(sm, a.sy);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    write_header(a.out, a.n, a.q1.eb_e);
-    if (chunks == 0) *a.out_size = HDR;
-  }
-  __syncthreads();
-  uint32_t phase = 0;
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= chunks) break;
-    store_body(sm, a, &map_in, c, chunks, phase);
-    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
-  }
-  finish_launch(sm, a.sy);
-}
-
-template <int OP>
-__global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
-  Smem& sm = smem_block();
-  StreamHdr h = read_header(a.in, a.in_bytes);
-  const bool hdr_ok = h.ok && h.n == a.n;
-  if (!hdr_ok) h.chunks = 0;
-  launch_prologue(sm, a.sy);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
-    write_header(a.out, hdr_ok ? h.n : 0, (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e);
-    if (h.chunks == 0) *a.out_size = HDR;
-  }
-  __syncthreads();
-  DecState ds{0, 0, 0};
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= h.chunks) break;
-    reencode_body<OP>(sm, a, h, ds, c);
-    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
-  }
-  finish_launch(sm, a.sy);
-}
-
-template <int OP>
-__global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
-                                               const __grid_constant__ CUtensorMap map_out) {
-  Smem& sm = smem_block();
-  StreamHdr h = read_header(a.in, a.in_bytes);
-  bool hdr_ok = h.ok && h.n <= a.out_cap;
-  if (OP == OP_RAPPLY) hdr_ok = hdr_ok && h.n == a.n;
-  if (!hdr_ok) h.chunks = 0;
-  launch_prologue(sm, a.sy);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
-    *a.out_size = hdr_ok ? h.n : 0;
-  }
-  __syncthreads();
-  DecState ds{0, 0, 0};
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= h.chunks) break;
-    decode_body<OP>(sm, a, h, ds, c, &map_src, &map_out);
-    if (threadIdx.x == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) bulk_wait_read();
-  finish_launch(sm, a.sy);
-}
-
-// ---- batched kernels: one persistent launch over many streams.
-// The queue index runs over the items' chunks back to back; each item has its
-// own lookback words (Sync.flags offset by its chunk base), header and size.
+// Many streams in one launch: the queue runs over the items' chunks back to
+// back; each item has its own lookback words (Sync.flags offset by its chunk
+// base), header and size.
 struct __align__(64) BatchItem {
   CUtensorMap map_in;   // store: the floats; resi_recv: the client's floats
   CUtensorMap map_out;  // decoders: the output floats
@@ -307,61 +157,548 @@ struct __align__(64) BatchItem {
   long long chunks;
 };
 
-// Item of queue index g (binary search over the items' chunk bases).
-__device__ __forceinline__ int find_item(const BatchItem* items, int n_items, long long g) {
-  int lo = 0, hi = n_items - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (items[mid].chunk_base <= g) lo = mid;
-    else hi = mid - 1;
+template <int OP>
+struct BatchSrc {
+  static constexpr bool batched = true;
+  const BatchItem* items;
+  int n_items;
+  long long total;
+  // Item of queue index g, searched by the whole warp forward from `cur` (the
+  // item of an earlier index of this CTA, or -1): 32 chunk bases per read.
+  __device__ __forceinline__ int locate(long long g, int cur, long long& c) const {
+    const int lane = threadIdx.x & 31;
+    int lo = cur < 0 ? 0 : cur;
+    while (true) {
+      const int i = lo + lane;
+      const bool le = i < n_items && items[i].chunk_base <= g;
+      const int cnt = __popc(__ballot_sync(0xffffffffu, le));
+      if (cnt < 32) {
+        const int it = lo + cnt - 1;
+        c = g - items[it].chunk_base;
+        return it;
+      }
+      lo += 31;
+    }
   }
-  return lo;
+  __device__ __forceinline__ const OpArgs& args(int i) const { return items[i].a; }
+  __device__ __forceinline__ const CUtensorMap* min(int i) const { return &items[i].map_in; }
+  __device__ __forceinline__ const CUtensorMap* mout(int i) const { return &items[i].map_out; }
+  __device__ __forceinline__ StreamHdr header(int i) const { return read_header(items[i].a.in, items[i].a.in_bytes); }
+  // 0 = usable; 2 = size mismatch; 3 = corrupt header
+  __device__ __forceinline__ int header_bad(int i, const StreamHdr& h) const {
+    const OpArgs& a = items[i].a;
+    if (!h.ok) return 3;
+    const bool ok = h.n == a.n && (OP == OP_S2C || OP == OP_RESI || h.n <= a.out_cap);
+    return ok ? 0 : 2;
+  }
+  // offset scanner over every usable item's size table, item after item
+  __device__ __forceinline__ void scan(unsigned int epoch) const {
+    for (int i = 0; i < n_items; i++) {
+      const StreamHdr h = header(i);
+      if (header_bad(i, h)) continue;
+      scan_offsets(items[i].a.sy.offs, epoch, reinterpret_cast<const uint16_t*>(items[i].a.in + HDR), h.chunks);
+    }
+  }
+};
+
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
+}
+
+// ---- prefetchers (warp 3): resolve queue index g and start its loads into
+// stage t.  Every TMA is issued by lane 0 (TMA_TID).
+struct WalkState {
+  int item;                 // item of the last prefetched index (-1: none)
+};
+
+template <class Src>
+__device__ __forceinline__ void prefetch_floats(Ctl& sm, int t, long long g, const Src& src, WalkState& ws) {
+  const int lane = threadIdx.x & 31;
+  StageMeta& m = sm.st[t];
+  if (g >= src.total) {
+    if (lane == 0) {
+      m.g = g;
+      mbar_arrive(&sm.bar[t]);
+      mbar_arrive(&sm.bar[t]);
+    }
+    return;
+  }
+  long long c;
+  const int item = src.locate(g, ws.item, c);
+  const bool fresh = item != ws.item;
+  ws.item = item;
+  if (lane == 0) {
+    const OpArgs& A = src.args(item);
+    const int nw = (int)min((long long)CW, (A.n - c * CS) / 4);
+    const bool tma = nw == CW && A.has_map_in;
+    if (tma) {
+      if (Src::batched && fresh) tensormap_acquire(src.min(item));
+      fence_proxy_async();
+      mbar_expect_tx(&sm.bar[t], CS);
+      tma_load_rows(stage_buf(sm, t), src.min(item), (int)(c * 128), &sm.bar[t]);
+    } else {
+      mbar_arrive(&sm.bar[t]);
+    }
+    m.g = g;
+    m.c = c;
+    m.item = item;
+    m.nw = nw;
+    m.tma = tma;
+    m.n = A.n;
+    m.chunks = (A.n + CS - 1) / CS;
+    m.bad = 0;
+    mbar_arrive(&sm.bar[t]);
+  }
+}
+
+// Decoders: the payload offset comes from the launch's offset scanner (the
+// prefix sum of the size table that the reference's decoders form per CTA,
+// d_s2c.h:98-106).  One bulk copy brings the payload's 16-byte-aligned span;
+// the lanes copy the ragged tail.
+template <class Src>
+__device__ __forceinline__ void prefetch_stream(Ctl& sm, int t, long long g, const Src& src, WalkState& ws) {
+  const int lane = threadIdx.x & 31;
+  StageMeta& m = sm.st[t];
+  if (g >= src.total) {
+    if (lane == 0) {
+      m.g = g;
+      mbar_arrive(&sm.bar[t]);
+      mbar_arrive(&sm.bar[t]);
+    }
+    return;
+  }
+  long long c;
+  const int item = src.locate(g, ws.item, c);
+  const bool fresh = item != ws.item;
+  ws.item = item;
+  const OpArgs& A = src.args(item);
+  const StreamHdr h = src.header(item);
+  const int hb = src.header_bad(item, h);
+  if (hb) {
+    if (lane == 0) {
+      m.g = g;
+      m.c = c;
+      m.item = item;
+      m.nw = CW;
+      m.tma = 0;
+      m.bad = hb;
+      m.csize = 0;
+      m.d = 0;
+      m.n = 0;
+      m.chunks = 0;
+      m.eb_e = 1;
+      mbar_arrive(&sm.bar[t]);
+      mbar_arrive(&sm.bar[t]);
+    }
+    return;
+  }
+  const long long chunks = h.chunks;
+  const int nw = (int)min((long long)CW, (h.n - c * CS) / 4);
+  const int osize = nw * 4;
+  const uint16_t* table = reinterpret_cast<const uint16_t*>(A.in + HDR);
+  const uint8_t* data = A.in + HDR + 2 * chunks;
+  const long long data_bytes = A.in_bytes - HDR - 2 * chunks;
+  unsigned long long off = 0;
+  if (lane == 0) off = wait_offset(A.sy, sm.epoch, c);
+  off = __shfl_sync(0xffffffffu, off, 0);
+  const int cs = table[c];
+  const int bad = (cs > osize) || (cs < 2 && cs != osize) || ((long long)off + cs > data_bytes);
+  const uintptr_t Aa = reinterpret_cast<uintptr_t>(data + off);
+  const uintptr_t a0 = Aa & ~uintptr_t(15);
+  uintptr_t a1 = (Aa + (bad ? 0 : cs)) & ~uintptr_t(15);
+  if (a1 < a0) a1 = a0;
+  const int d = (int)(Aa - a0);
+  const int tma_len = (int)(a1 - a0);
+  uint8_t* dst = reinterpret_cast<uint8_t*>(stage_buf(sm, t));
+  if (lane == 0) {
+    bulk_wait_read();  // a TMA store of this buffer's previous chunk may still be reading it
+    fence_proxy_async();
+    if (tma_len) {
+      if (Src::batched && fresh) tensormap_acquire(src.mout(item));
+      mbar_expect_tx(&sm.bar[t], (uint32_t)tma_len);
+      bulk_load(dst, reinterpret_cast<const void*>(a0), (uint32_t)tma_len, &sm.bar[t]);
+    } else {
+      if (Src::batched && fresh) tensormap_acquire(src.mout(item));
+      mbar_arrive(&sm.bar[t]);
+    }
+    if (Src::batched && fresh) tensormap_acquire(src.min(item));
+    m.g = g;
+    m.c = c;
+    m.item = item;
+    m.nw = nw;
+    m.tma = tma_len != 0;
+    m.bad = bad;
+    m.csize = bad ? 0 : cs;
+    m.d = d;
+    m.tma_len = tma_len;
+    m.off = off;
+    m.n = h.n;
+    m.chunks = chunks;
+    m.eb_e = h.eb_e;
+  }
+  __syncwarp();
+  if (!bad) {
+    const uint8_t* gsrc = data + off;
+    const int from = tma_len - d;  // payload bytes [from, cs) are copied by the lanes
+    for (int i = lane + (from > 0 ? from : 0); i < cs; i += 32) dst[d + i] = gsrc[i];
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&sm.bar[t]);
+}
+
+// ---- the three pipelined loops.  Each CTA dequeues chunk indices from the
+// launch's queue; warp 3 resolves an index and starts its loads.  Decoders
+// take their indices one iteration ahead and load the next chunk while the
+// current one is decoded; encoders take an index when they start the chunk.
+//
+// Encoders publish a chunk's compressed size as soon as it is known and write
+// its payload one iteration later (flush_chunk): by then every earlier chunk
+// has published too, and the resolver CTA has usually turned the chunk's own
+// lookback word into an inclusive prefix, so no CTA waits on its
+// predecessors while it holds the SM.
+
+// Resolves and writes out the chunk pending in stage t (if any): warp 0 finds
+// its output offset, a barrier publishes it, every thread stores the payload.
+// Called by every thread.
+template <class Src, typename RawWordOf>
+__device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, const uint32_t* staging, bool raw_staged,
+                                              RawWordOf raw_word_of) {
+  Pend& pd = sm.pend[t];
+  const bool valid = pd.valid;  // written before an earlier barrier
+  if (valid && threadIdx.x < 32) {
+    const unsigned long long X = lookback_resolve(src.args(pd.item).sy, sm.epoch, pd.c, pd.csize);
+    if (threadIdx.x == 0) sm.payload_off = X;
+  }
+  __syncthreads();
+  if (valid) {
+    const OpArgs& Q = src.args(pd.item);
+    const long long chunks = (Q.n + CS - 1) / CS;
+    flush_chunk(sm, pd, staging, raw_staged, raw_word_of(Q, pd.c), Q.out + HDR + 2 * chunks,
+                reinterpret_cast<uint16_t*>(Q.out + HDR), Q.out_size, chunks);
+  }
+}
+
+// store (d_server_encode_kernel): floats -> SQ -> encode.  A chunk arrives in
+// stage buffer s, becomes its plane buffer and then its staging; the previous
+// chunk's staging (buffer s^1) is flushed once this chunk's size is
+// published, and the next chunk is then loaded into buffer s^1.
+template <class Src>
+__device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& sy) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  begin_launch(sm, sy);
+  if (tid == 0) {
+    sm.pend[0].valid = 0;
+    sm.pend[1].valid = 0;
+  }
+  WalkState ws{-1};
+  __syncthreads();
+  // a raw chunk stores the original floats, read again from global memory
+  auto raw_word_of = [](const OpArgs& Q, long long c) {
+    const uint32_t* gin = reinterpret_cast<const uint32_t*>(Q.in) + c * (long long)CW;
+    return [gin](int w) -> uint32_t { return gin[w]; };
+  };
+  auto take_next = [&](int t) {
+    if (warp == 3) {
+      long long g = 0;
+      if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
+      prefetch_floats(sm, t, __shfl_sync(0xffffffffu, g, 0), src, ws);
+    }
+  };
+  take_next(0);
+  uint32_t phase = 0;  // bit s: parity of stage s's barrier
+  int s = 0;
+  for (;; s ^= 1) {
+    if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u << s;
+    const StageMeta& m = sm.st[s];
+    if (m.g >= src.total) break;
+    const int item = m.item;
+    const OpArgs& A = src.args(item);
+    const long long c = m.c;
+    const int nw = m.nw;
+    uint32_t* buf = stage_buf(sm, s);
+    if (!m.tma) {
+      load_plain_rows(buf, A.in, c, nw);
+      __syncthreads();
+    }
+    if (Src::batched && c == 0 && tid == 0) write_header(A.out, A.n, A.q1.eb_e);
+    uint32_t v[32];
+    row_load(buf, tid, v);
+    const Quant q1 = A.q1;
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], q1);
+    uint32_t* prev_buf = stage_buf(sm, s ^ 1);
+    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, prev_buf, false, raw_word_of); };
+    if (nw == CW) {
+      encode_stage<true>(sm, A.sy, v, buf, nullptr, c, nw, item, sm.pend[s], flush_prev);
+    } else {
+      encode_stage_partial(sm, A.sy, v, buf, nullptr, c, nw, item, sm.pend[s]);
+      flush_prev();
+    }
+    if (tid == 0) sm.pend[s ^ 1].valid = 0;
+    __syncthreads();  // buffer s^1 has been flushed and can take the next chunk
+    take_next(s ^ 1);
+  }
+  flush_pending(sm, src, s ^ 1, stage_buf(sm, s ^ 1), false, raw_word_of);
+}
+
+// init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
+// decode the stored chunk, requantize or form the residual, encode.  The
+// payload arrives in buffer 0 (which then holds the requantized words for the
+// raw fallback); buffers 1 and 2 alternate as the plane buffer of both halves
+// and the staging that waits for the flush.
+template <int OP, class Src>
+__device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Sync& sy) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  begin_launch(sm, sy);
+  if (tid == 0) {
+    sm.pend[0].valid = 0;
+    sm.pend[1].valid = 0;
+  }
+  WalkState ws{-1};
+  __syncthreads();  // sm.epoch
+  if (gridDim.x == 1 && warp == 1) src.scan(sm.epoch);
+  __syncthreads();
+  auto raw_word_of = [](const OpArgs&, long long) { return [](int) -> uint32_t { return 0u; }; };
+  auto take_next = [&]() {
+    if (warp == 3) {
+      long long g = 0;
+      if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
+      prefetch_stream(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
+    }
+  };
+  take_next();
+  uint32_t* P = stage_buf(sm, 0);
+  uint32_t phase = 0;
+  int s = 0;
+  for (;; s ^= 1) {
+    uint32_t* C = stage_buf(sm, 1 + s);
+    uint32_t* Cprev = stage_buf(sm, 2 - s);
+    if (!mbar_wait(&sm.bar[0], phase & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u;
+    const StageMeta& m = sm.st[0];
+    if (m.g >= src.total) break;
+    const int item = m.item;
+    const OpArgs& A = src.args(item);
+    const long long c = m.c;
+    const int nw = m.nw;
+    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, Cprev, true, raw_word_of); };
+    uint32_t v[32];
+    bool raw;
+    if (nw == CW) decode_core<true>(sm, A.sy, m, P, C, v, raw, NoHook{});
+    else decode_core_partial(sm, A.sy, m, P, C, v, raw, NoHook{});
+    if (m.bad >= 2) {  // unusable stream header (batched): nothing to write
+      if (tid == 0) sm.pend[s].valid = 0;
+      flush_prev();
+    } else {
+      // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
+      // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
+      const Quant qs = make_quant(m.eb_e);
+      const Quant q1 = A.q1, q2 = A.q2;
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+        if (OP == OP_S2C) {
+          v[k] = cq_enc(x, q1);
+        } else {
+          const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
+          v[k] = cq_enc(x, q2) - src_req;
+        }
+      }
+      row_store(P, tid, v);  // raw source: the bins / residuals
+      if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
+      if (nw == CW) {
+        encode_stage<true>(sm, A.sy, v, C, P, c, nw, item, sm.pend[s], flush_prev);
+      } else {
+        encode_stage_partial(sm, A.sy, v, C, P, c, nw, item, sm.pend[s]);
+        flush_prev();
+      }
+    }
+    if (tid == 0) sm.pend[s ^ 1].valid = 0;
+    __syncthreads();  // buffer 0 (payload, raw copy) and the flushed staging are free
+    take_next();
+  }
+  flush_pending(sm, src, s ^ 1, stage_buf(sm, 2 - s), true, raw_word_of);
+}
+
+// storage decode / init_recv / resi_recv (d_server_decode_kernel,
+// d_client_decode_kernel, d_residual_apply_kernel).  The payload is expanded
+// in place in its stage buffer, which then stages the output floats for one
+// TMA store; resi_recv's client chunk arrives in buffer 2.
+template <int OP, class Src>
+__device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync& sy) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  begin_launch(sm, sy);
+  __syncthreads();
+  if (gridDim.x == 1 && warp == 1) src.scan(sm.epoch);
+  __syncthreads();
+  WalkState ws{-1};
+  long long pending = 0;
+  if (warp == 3) {
+    long long g0 = 0;
+    if (lane == 0) g0 = atomicAdd(&sy.counter[0], 1u);
+    g0 = __shfl_sync(0xffffffffu, g0, 0);
+    prefetch_stream(sm, 0, g0, src, ws);
+    if (lane == 0) pending = atomicAdd(&sy.counter[0], 1u);
+  }
+  __syncthreads();
+  uint32_t* S = stage_buf(sm, 2);
+  uint32_t phase = 0;  // bits 0, 1: stages; bit 2: client chunk
+  for (int s = 0;; s ^= 1) {
+    const StageMeta& m = sm.st[s];
+    if (m.g >= src.total) break;
+    const int item = m.item;
+    const OpArgs& A = src.args(item);
+    const long long c = m.c;
+    const int nw = m.nw;
+    const bool full = nw == CW;
+    uint32_t* P = stage_buf(sm, s);
+    bool src_tma = false;
+    if (OP == OP_RAPPLY && m.bad < 2) {
+      src_tma = full && A.has_map_in;
+      if (src_tma) {
+        if (tid == TMA_TID) {
+          fence_proxy_async();
+          mbar_expect_tx(&sm.bar_src, CS);
+          tma_load_rows(S, src.min(item), (int)(c * 128), &sm.bar_src);
+        }
+      } else {
+        load_plain_rows(S, A.src, c, nw);  // visible after the decoder's barriers
+      }
+    }
+    if (Src::batched && c == 0 && tid == 0 && m.bad < 2) *A.out_size = m.n;
+    if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u << s;
+    auto next = [&]() {
+      if (warp == 3) {
+        const long long gp = __shfl_sync(0xffffffffu, pending, 0);
+        if (lane == 0) pending = atomicAdd(&sy.counter[0], 1u);
+        prefetch_stream(sm, s ^ 1, gp, src, ws);
+      }
+    };
+    uint32_t v[32];
+    bool raw;
+    if (full) {
+      decode_core<true>(sm, A.sy, m, P, P, v, raw, next);
+    } else {
+      next();
+      decode_core_partial(sm, A.sy, m, P, P, v, raw, NoHook{});
+    }
+    if (m.bad >= 2) {  // unusable stream header (batched): nothing to write
+      __syncthreads();
+      continue;
+    }
+    const Quant q = make_quant(m.eb_e);
+    if (OP == OP_RAPPLY) {
+      // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
+      // destination bound, add the residual, dequantize.
+      if (src_tma) {
+        if (!mbar_wait(&sm.bar_src, (phase >> 2) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+        phase ^= 4u;
+      }
+      uint32_t s2[32];
+      row_load(S, tid, s2);
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s2[k], q) + v[k], q);
+    } else if (!raw) {
+      // chunks stored uncompressed are copied out as stored: original floats
+      // for storage decode (d_server_encode.h:234-249), request bins for
+      // init_recv (d_client_encode.h:230-254, the reference's behaviour)
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
+    }
+    row_store(P, tid, v);  // every plane read finished before the decoder's last barrier
+    const bool tma_out = full && A.has_map_out;
+    if (tma_out) fence_proxy_async();
+    __syncthreads();
+    if (tma_out) {
+      if (tid == TMA_TID) {
+        tma_store_rows(src.mout(item), (int)(c * 128), P);
+        bulk_commit();
+      }
+    } else {
+      uint32_t* g = reinterpret_cast<uint32_t*>(A.out) + c * (long long)CW;
+      for (int w = tid; w < nw; w += NT) g[w] = P[swz(w)];
+      __syncthreads();
+    }
+  }
+  if (tid == TMA_TID) bulk_wait_read();
+}
+
+// ---- the helper CTA of a launch (its last CTA, when there are at least two):
+// warp 0 runs the lookback resolver (encoders), warp 1 the offset scanner
+// (stream inputs).  A one-CTA launch scans its offsets itself first.
+__device__ __forceinline__ bool helper_cta() { return gridDim.x >= 2 && blockIdx.x == gridDim.x - 1; }
+
+template <bool RESOLVE, bool SCAN, class Src>
+__device__ __forceinline__ void run_helper(Ctl& sm, const Src& src, const Sync& sy) {
+  begin_launch(sm, sy);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  if (RESOLVE && warp == 0) resolve_loop(sy, sm.epoch, src.total);
+  if (SCAN && warp == 1) src.scan(sm.epoch);
+}
+
+// ---- single-stream kernels
+__global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
+  Ctl& sm = ctl_block();
+  const long long chunks = (a.n + CS - 1) / CS;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    write_header(a.out, a.n, a.q1.eb_e);
+    if (chunks == 0) *a.out_size = HDR;
+  }
+  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
+  if (helper_cta()) run_helper<true, false>(sm, src, a.sy);
+  else store_loop(sm, src, a.sy);
+  finish_launch(sm, a.sy);
 }
 
 template <int OP>
+__global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
+  Ctl& sm = ctl_block();
+  StreamHdr h = read_header(a.in, a.in_bytes);
+  const bool hdr_ok = h.ok && h.n == a.n;
+  if (!hdr_ok) h.chunks = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
+    write_header(a.out, hdr_ok ? h.n : 0, (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e);
+    if (h.chunks == 0) *a.out_size = HDR;
+  }
+  const SingleSrc src{&a, nullptr, nullptr, h.chunks, h};
+  if (helper_cta()) run_helper<true, true>(sm, src, a.sy);
+  else reencode_loop<OP>(sm, src, a.sy);
+  finish_launch(sm, a.sy);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) k_decode(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_src,
+                                               const __grid_constant__ CUtensorMap map_out) {
+  Ctl& sm = ctl_block();
+  StreamHdr h = read_header(a.in, a.in_bytes);
+  bool hdr_ok = h.ok && h.n <= a.out_cap;
+  if (OP == OP_RAPPLY) hdr_ok = hdr_ok && h.n == a.n;
+  if (!hdr_ok) h.chunks = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
+    *a.out_size = hdr_ok ? h.n : 0;
+  }
+  const SingleSrc src{&a, &map_src, &map_out, h.chunks, h};
+  if (helper_cta()) run_helper<false, true>(sm, src, a.sy);
+  else decode_loop<OP>(sm, src, a.sy);
+  finish_launch(sm, a.sy);
+}
+
+// ---- batched kernels: one persistent launch over many streams.
+template <int OP>
 __global__ void __launch_bounds__(NT, OP == OP_STORE ? MINB_STORE : (OP == OP_RAPPLY ? MINB_RAPPLY : (OP == OP_S2C || OP == OP_RESI) ? MINB_REENC : MINB_DEC))
 k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks, const __grid_constant__ Sync sy) {
-  Smem& sm = smem_block();
-  launch_prologue(sm, sy);
-  __syncthreads();
-  uint32_t phase = 0;
-  DecState ds{0, 0, 0};
-  int cur = -1;
-  while (true) {
-    const long long g = sm.chunk;
-    if (g >= total_chunks) break;
-    const int i = find_item(items, n_items, g);
-    const BatchItem& it = items[i];
-    const long long c = g - it.chunk_base;
-    if (i != cur) {  // a new stream: reset the decoders' running offset
-      cur = i;
-      ds.prev_c = 0;
-      ds.prev_off = 0;
-      if (threadIdx.x == 0) {
-        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&it.map_in) : "memory");
-        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&it.map_out) : "memory");
-      }
-    }
-    if (OP == OP_STORE) {
-      if (c == 0 && threadIdx.x == 0) write_header(it.a.out, it.a.n, it.a.q1.eb_e);
-      store_body(sm, it.a, &it.map_in, c, it.chunks, phase);
-    } else {
-      StreamHdr h = read_header(it.a.in, it.a.in_bytes);
-      const bool ok = h.ok && h.n == it.a.n && (OP == OP_S2C || OP == OP_RESI || h.n <= it.a.out_cap);
-      if (!ok) {
-        if (threadIdx.x == 0) latch(sy.status, !h.ok ? DST_CORRUPT : DST_SIZE_MISMATCH);
-      } else if (OP == OP_S2C || OP == OP_RESI) {
-        if (c == 0 && threadIdx.x == 0) write_header(it.a.out, h.n, (OP == OP_S2C) ? it.a.q1.eb_e : it.a.q2.eb_e);
-        reencode_body<OP>(sm, it.a, h, ds, c);
-      } else {
-        if (c == 0 && threadIdx.x == 0) *it.a.out_size = h.n;
-        decode_body<OP>(sm, it.a, h, ds, c, &it.map_in, &it.map_out);
-      }
-    }
-    if (threadIdx.x == 0) sm.chunk = atomicAdd(&sy.counter[0], 1u);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) bulk_wait_read();
+  Ctl& sm = ctl_block();
+  const BatchSrc<OP> src{items, n_items, total_chunks};
+  constexpr bool encoder = OP == OP_STORE || OP == OP_S2C || OP == OP_RESI;
+  if (helper_cta()) run_helper<encoder, OP != OP_STORE>(sm, src, sy);
+  else if (OP == OP_STORE) store_loop(sm, src, sy);
+  else if (encoder) reencode_loop<OP>(sm, src, sy);
+  else decode_loop<OP>(sm, src, sy);
   finish_launch(sm, sy);
 }
 
@@ -378,51 +715,15 @@ __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_CHUNKS + 
 // clears the status word for the next call (finish_launch).
 __global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_constant__ OpArgs a,
                                                                   const __grid_constant__ CUtensorMap map_in) {
-  Smem& sm = smem_block();
-  const int tid = threadIdx.x;
-  const long long n = a.n;
-  const long long chunks = (n + CS - 1) / CS;
-  begin_launch(sm, a.sy);
-  if (tid == 0) {
-    mbar_init(&sm.bar, 1);
-    fence_mbar_init();
-    sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-  }
-  if (blockIdx.x == 0 && tid == 0) {
-    *reinterpret_cast<long long*>(a.out) = n;
-    reinterpret_cast<int*>(a.out)[2] = a.q1.eb_e;
-    reinterpret_cast<int*>(a.out)[3] = 0;
+  Ctl& sm = ctl_block();
+  const long long chunks = (a.n + CS - 1) / CS;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    write_header(a.out, a.n, a.q1.eb_e);
     if (chunks == 0) *a.out_size = HDR;
   }
-  __syncthreads();
-  uint16_t* table = reinterpret_cast<uint16_t*>(a.out + HDR);
-  uint8_t* data = a.out + HDR + 2 * chunks;
-  uint32_t phase = 0;
-  while (true) {
-    const long long c = sm.chunk;
-    if (c >= chunks) break;
-    const int nw = (int)min((long long)CW, (n - c * CS) / 4);
-    if (nw == CW && a.has_map_in) {
-      if (tid == 0) {
-        fence_proxy_async();
-        mbar_expect_tx(&sm.bar, CS);
-        tma_load_rows(sm.buf0, &map_in, (int)(c * 128), &sm.bar);
-      }
-      if (!mbar_wait(&sm.bar, phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
-      phase ^= 1;
-    } else {
-      load_plain_rows(sm.buf0, a.in, c, nw);
-      __syncthreads();
-    }
-    uint32_t v[32];
-    row_load(sm.buf0, tid, v);
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], a.q1);
-    if (nw == CW) encode_chunk<true>(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-    else encode_chunk_partial(sm, a, v, sm.buf0, c, nw, chunks, data, table);
-    if (tid == 0) sm.chunk = atomicAdd(&a.sy.counter[0], 1u);
-    __syncthreads();
-  }
+  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
+  if (helper_cta()) run_helper<true, false>(sm, src, a.sy);
+  else store_loop(sm, src, a.sy);
   const unsigned int st = finish_launch(sm, a.sy, true);
   if (st) *a.out_size = -(long long)st;
 }
@@ -559,9 +860,10 @@ cortado_status ensure_flags(cortado_ctx* ctx, int64_t chunks, cudaStream_t st) {
     ctx->flags = nullptr;
     ctx->flags_cap = 0;
   }
-  cudaError_t e = cudaMalloc(&ctx->flags, (size_t)cap * 8);
+  // lookback words, then the input payload offsets
+  cudaError_t e = cudaMalloc(&ctx->flags, (size_t)cap * 16);
   if (e != cudaSuccess) return from_cuda(e);
-  e = cudaMemsetAsync(ctx->flags, 0, (size_t)cap * 8, st);
+  e = cudaMemsetAsync(ctx->flags, 0, (size_t)cap * 16, st);
   if (e != cudaSuccess) return from_cuda(e);
   ctx->flags_cap = cap;
   return CORTADO_OK;
@@ -570,6 +872,7 @@ cortado_status ensure_flags(cortado_ctx* ctx, int64_t chunks, cudaStream_t st) {
 Sync next_sync(cortado_ctx* ctx, cudaStream_t) {
   Sync s;
   s.flags = ctx->flags;
+  s.offs = ctx->flags + ctx->flags_cap;
   s.flags_cap = ctx->flags_cap;
   s.counter = ctx->words;
   s.status = ctx->words + 2;
@@ -602,8 +905,8 @@ int occupancy_grid(K kernel, size_t smem, int sms) {
   return per * sms;
 }
 
-constexpr size_t SMEM_STD = SMEM_BYTES + 1024;           // + alignment slack
-constexpr size_t SMEM_SRC = SMEM_BYTES + CS + 1024;      // resi_recv: + client chunk
+constexpr size_t SMEM_STD = smem_bytes(2);  // store, storage decode, init_recv
+constexpr size_t SMEM_SRC = smem_bytes(3);  // init_send, resi_send, resi_recv
 
 cortado_status launch_status(cudaError_t e) { return from_cuda(e == cudaSuccess ? cudaGetLastError() : e); }
 
@@ -654,14 +957,14 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   if (e != cudaSuccess) { delete ctx; return from_cuda(e); }
   cudaMemset(ctx->words, 0, 64);
   ctx->grid_store = occupancy_grid(k_store, SMEM_STD, ctx->sms);
-  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_STD, ctx->sms);
-  occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
+  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_SRC, ctx->sms);
+  occupancy_grid(k_reencode<OP_RESI>, SMEM_SRC, ctx->sms);
   ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
   occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_SRC, ctx->sms);
   ctx->grid_batch[OP_STORE] = occupancy_grid(k_batch<OP_STORE>, SMEM_STD, ctx->sms);
-  ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_STD, ctx->sms);
-  ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_SRC, ctx->sms);
+  ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_SRC, ctx->sms);
   ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_SRC, ctx->sms);
@@ -761,8 +1064,8 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.q2 = make_quant(e2);
   a.sy = next_sync(ctx, st);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
-  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
-  else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
+  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_SRC, st>>>(a);
+  else k_reencode<OP_RESI><<<grid, NT, SMEM_SRC, st>>>(a);
   return launch_status(cudaSuccess);
 }
 
@@ -785,6 +1088,9 @@ static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int
   if (!ctx || !d_stream || !d_out || !d_outsize || stream_bytes < HDR || out_capacity < 0) return CORTADO_ERR_INVALID_ARG;
   if (!aligned16(d_stream) || !aligned16(d_out) || (d_src && !aligned16(d_src))) return CORTADO_ERR_ALIGNMENT;
   cudaStream_t st = (cudaStream_t)stream;
+  const int64_t chunk_bound = chunks_of(op == OP_RAPPLY ? n_bytes : out_capacity);
+  cortado_status es = ensure_flags(ctx, chunk_bound, st);
+  if (es) return es;
   OpArgs a{};
   a.in = (const uint8_t*)d_stream;
   a.in_bytes = stream_bytes;
@@ -801,7 +1107,6 @@ static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int
   // the kernel checks lie inside the header's size).
   a.has_map_out = make_rows_map(&mout, d_out, op == OP_RAPPLY ? n_bytes : out_capacity);
   if (op == OP_RAPPLY) a.has_map_in = make_rows_map(&msrc, d_src, n_bytes);
-  const int64_t chunk_bound = chunks_of(op == OP_RAPPLY ? n_bytes : out_capacity);
   if (op == OP_SDEC) k_decode<OP_SDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
   else if (op == OP_CDEC) k_decode<OP_CDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
   else k_decode<OP_RAPPLY><<<grid_for(tuned_grid(ctx, op, ctx->grid_rapply), chunk_bound), NT, SMEM_SRC, st>>>(a, msrc, mout);
@@ -948,6 +1253,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
     a.q2 = make_quant(e2);
     a.sy = sy;
     a.sy.flags = sy.flags + base;
+    a.sy.offs = sy.offs + base;
     if (op == CORTADO_OP_STORE) a.has_map_in = make_rows_map(&b.map_in, it.d_in, it.n_bytes);
     if (op == CORTADO_OP_RESI_RECV) a.has_map_in = make_rows_map(&b.map_in, it.d_src, it.n_bytes);
     if (op == CORTADO_OP_STORE_DECODE || op == CORTADO_OP_INIT_RECV || op == CORTADO_OP_RESI_RECV)
@@ -959,7 +1265,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   cudaError_t e = cudaMemcpyAsync(d_tab, h_tab, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return from_cuda(e);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_batch[op]), total);
-  const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_SRC : SMEM_STD;
+  const size_t smem = (op == CORTADO_OP_RESI_RECV || op == CORTADO_OP_INIT_SEND || op == CORTADO_OP_RESI_SEND) ? SMEM_SRC : SMEM_STD;
   switch (op) {
     case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
     case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
@@ -1020,6 +1326,7 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
   a.n = n_bytes;
   a.q1 = make_quant(e);
   a.sy.flags = d.scratch;
+  a.sy.offs = nullptr;
   a.sy.flags_cap = NOALLOC_CHUNKS;
   a.sy.counter = reinterpret_cast<unsigned int*>(d.scratch + NOALLOC_CHUNKS);
   a.sy.status = a.sy.counter + 2;

@@ -54,7 +54,8 @@ __host__ __device__ inline Quant make_quant(int eb_e) {
 // get a fresh epoch on every replay.
 struct Sync {
   unsigned long long* flags;  // lookback words, one per chunk (encoders)
-  long long flags_cap;        // words in flags (cleared when the epoch wraps)
+  unsigned long long* offs;   // input payload offsets, one per chunk (decoders, re-encoders), or null
+  long long flags_cap;        // words in flags and in offs (cleared when the epoch wraps)
   unsigned int* counter;      // [0] chunk queue, [1] CTAs finished
   unsigned int* status;       // first error latched
   unsigned int* epoch;        // 0..65535, tags this launch's lookback words
@@ -96,6 +97,11 @@ __device__ __forceinline__ void fence_mbar_init() {
 }
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Plain arrival (no transaction bytes): release semantics, so the arriving
+// thread's earlier shared-memory writes are visible to the waiters.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -299,13 +305,21 @@ constexpr unsigned long long LB_AGG = 1ull << 46, LB_INC = 2ull << 46, LB_VAL = 
 
 // Decoupled lookback over the chunk sizes (the role of propagate_carry,
 // include/d_compression.h:120-160).  Called by one whole warp; returns the
-// exclusive prefix of compressed bytes before chunk c.  Each poll reads the 32
-// nearest unaccounted predecessors (one per lane); once all have published,
-// the nearest inclusive prefix ends the walk, otherwise their sizes are added
-// and the window moves 32 chunks back.  Every wait is bounded: on timeout, or
-// when another CTA has already failed, the launch's status is set and 0 is
-// returned.  lookback_published expects chunk c's own word to be published
-// already (lookback_publish), so a caller can do other work in between.
+// exclusive prefix of compressed bytes before chunk c.  Each poll reads the
+// LB_WIN nearest unaccounted predecessors (LB_PER per lane, lane l covering
+// distances l*LB_PER .. l*LB_PER+LB_PER-1 from the window top).  The walk ends
+// at the nearest inclusive prefix if every word nearer than it has been
+// published; if the whole window holds published aggregates, they are added
+// and the window moves LB_WIN chunks back; otherwise the window is read
+// again.  (Wider windows were measured slower: a poll that waits for a
+// predecessor re-reads the whole window, and that traffic delays everyone.)
+// Every wait is bounded: on timeout, or when another CTA has already failed,
+// the launch's status is set and 0 is returned.  lookback_published expects
+// chunk c's own word to be published already (lookback_publish), so a caller
+// can do other work in between.
+constexpr int LB_PER = 1;
+constexpr int LB_WIN = 32 * LB_PER;
+
 __device__ __forceinline__ unsigned long long lookback_published(const Sync& sy, unsigned int epoch, long long c,
                                                                  unsigned int csize) {
   const int lane = threadIdx.x & 31;
@@ -314,32 +328,54 @@ __device__ __forceinline__ unsigned long long lookback_published(const Sync& sy,
   unsigned long long excl = 0;
   long long top = c - 1;
   const unsigned long long t0 = globaltimer();
+  int spins = 0;
   while (true) {
-    const long long idx = top - lane;
-    unsigned long long f = 0;
-    int spins = 0;
-    while (true) {
-      f = (idx >= 0) ? ld_relaxed(&sy.flags[idx]) : (tag | LB_INC);
-      const bool ready = ((f >> 48) == epoch) && ((f & (3ull << 46)) != 0);
-      if (__all_sync(0xffffffffu, ready)) break;
-      if ((++spins & 31) == 0) {
-        int bad = 0;
-        if (lane == 0) bad = (globaltimer() - t0 > sy.timeout_ns) || (*(volatile unsigned int*)sy.status != 0);
-        bad = __shfl_sync(0xffffffffu, bad, 0);
-        if (bad) {
-          if (lane == 0) latch(sy.status, DST_TIMEOUT);
-          return 0;
-        }
-      }
+    // this lane's LB_PER words, nearest first
+    unsigned long long f[LB_PER];
+#pragma unroll
+    for (int j = 0; j < LB_PER; j++) {
+      const long long idx = top - (lane * LB_PER + j);
+      f[j] = (idx >= 0) ? ld_relaxed(&sy.flags[idx]) : (tag | LB_INC);
     }
-    const unsigned int inc = __ballot_sync(0xffffffffu, (f & LB_INC) != 0);
-    if (inc) {
-      const int p = __ffs(inc) - 1;
-      excl += warp_sum64(lane <= p ? (f & LB_VAL) : 0ull);
+    int fnr = LB_PER, finc = LB_PER;  // first word not ready / first inclusive word
+    unsigned long long all = 0, upto = 0;
+#pragma unroll
+    for (int j = LB_PER - 1; j >= 0; j--) {
+      const bool ready = ((f[j] >> 48) == epoch) && ((f[j] & (3ull << 46)) != 0);
+      if (!ready) fnr = j;
+      if (ready && (f[j] & LB_INC)) finc = j;
+    }
+#pragma unroll
+    for (int j = 0; j < LB_PER; j++) {
+      const unsigned long long val = f[j] & LB_VAL;
+      all += val;
+      if (j <= finc) upto += val;
+    }
+    const unsigned int nr_mask = __ballot_sync(0xffffffffu, fnr < LB_PER);
+    const unsigned int inc_mask = __ballot_sync(0xffffffffu, finc < LB_PER);
+    const int pn = nr_mask ? __ffs(nr_mask) - 1 : 32;
+    const int pi = inc_mask ? __ffs(inc_mask) - 1 : 32;
+    const int fnr_pn = __shfl_sync(0xffffffffu, fnr, pn & 31);
+    const int finc_pi = __shfl_sync(0xffffffffu, finc, pi & 31);
+    const bool inc_first = pi < 32 && (pi < pn || (pi == pn && finc_pi < fnr_pn));
+    if (inc_first) {
+      excl += warp_sum64(lane < pi ? all : (lane == pi ? upto : 0ull));
       break;
     }
-    excl += warp_sum64(f & LB_VAL);
-    top -= 32;
+    if (pn == 32) {  // every word of the window is a published aggregate
+      excl += warp_sum64(all);
+      top -= LB_WIN;
+      continue;
+    }
+    if ((++spins & 15) == 0) {
+      int bad = 0;
+      if (lane == 0) bad = (globaltimer() - t0 > sy.timeout_ns) || (*(volatile unsigned int*)sy.status != 0);
+      bad = __shfl_sync(0xffffffffu, bad, 0);
+      if (bad) {
+        if (lane == 0) latch(sy.status, DST_TIMEOUT);
+        return 0;
+      }
+    }
   }
   if (lane == 0) st_relaxed(&sy.flags[c], tag | LB_INC | (excl + csize));
   return excl;
@@ -356,6 +392,164 @@ __device__ __forceinline__ unsigned long long lookback(const Sync& sy, unsigned 
                                                        unsigned int csize) {
   if ((threadIdx.x & 31) == 0) lookback_publish(sy, epoch, c, csize);
   return lookback_published(sy, epoch, c, csize);
+}
+
+// Exclusive output offset of chunk c whose size was published a while ago:
+// one read of its own word, which the resolver (or the chunk's predecessors'
+// walks) has usually made inclusive by then; otherwise the ordinary walk.
+__device__ __forceinline__ unsigned long long lookback_resolve(const Sync& sy, unsigned int epoch, long long c,
+                                                               unsigned int csize) {
+  const unsigned long long f = ld_relaxed(&sy.flags[c]);
+  if ((f >> 48) == epoch && (f & LB_INC)) return (f & LB_VAL) - csize;
+  return lookback_published(sy, epoch, c, csize);
+}
+
+// The resolver: one warp that walks the lookback words of a launch in order
+// and turns every published aggregate into an inclusive prefix (running sum
+// since the last inclusive word; each stream's chunk 0 publishes an inclusive
+// word, so streams of a batched launch restart the sum by themselves).  It
+// reads 256 words per pass and converts the published run at the front of
+// them.  It stops at the end of the words or once every other CTA of the
+// launch has finished; it never latches an error (the chunks' own walks still
+// bound their waits).
+__device__ __forceinline__ void resolve_loop(const Sync& sy, unsigned int epoch, long long total) {
+  constexpr int PER = 8;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long tag = (unsigned long long)epoch << 48;
+  long long F = 0;
+  unsigned long long P = 0;  // inclusive prefix of chunk F-1
+  const unsigned long long t0 = globaltimer();
+  while (F < total) {
+    unsigned long long f[PER];
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const long long idx = F + lane * PER + j;
+      f[j] = idx < total ? ld_relaxed(&sy.flags[idx]) : 0ull;
+    }
+    int nr = PER;
+#pragma unroll
+    for (int j = PER - 1; j >= 0; j--)
+      if (!(((f[j] >> 48) == epoch) && ((f[j] & (3ull << 46)) != 0))) nr = j;
+    const unsigned int m = __ballot_sync(0xffffffffu, nr < PER);
+    const int pl = m ? __ffs(m) - 1 : 32;
+    const int R = pl < 32 ? pl * PER + __shfl_sync(0xffffffffu, nr, pl) : 32 * PER;
+    if (R == 0) {
+      int stop = 0;
+      if (lane == 0)
+        stop = (*(volatile unsigned int*)&sy.counter[1] >= gridDim.x - 1) || (globaltimer() - t0 > 4 * sy.timeout_ns);
+      if (__shfl_sync(0xffffffffu, stop, 0)) return;
+      __nanosleep(256);
+      continue;
+    }
+    // lane segment: positions lane*PER .. lane*PER+PER-1 below R
+    const int lim = min(PER, max(0, R - lane * PER));
+    bool reset = false;
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (j < lim) {
+        const unsigned long long v = f[j] & LB_VAL;
+        if (f[j] & LB_INC) {
+          reset = true;
+          sum = v;
+        } else {
+          sum += v;
+        }
+      }
+    }
+    // inclusive segmented scan of (reset, sum) over the lanes
+    bool r_in = reset;
+    unsigned long long s_in = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long s_up = __shfl_up_sync(0xffffffffu, s_in, o);
+      const int r_up = __shfl_up_sync(0xffffffffu, (int)r_in, o);
+      if (lane >= o && !r_in) {
+        s_in += s_up;
+        r_in = r_up;
+      }
+    }
+    // exclusive carry into this lane: the previous lane's inclusive value, or P
+    unsigned long long carry = __shfl_up_sync(0xffffffffu, s_in, 1);
+    const int carry_r = __shfl_up_sync(0xffffffffu, (int)r_in, 1);
+    if (lane == 0 || !carry_r) carry = (lane == 0 ? 0ull : carry) + P;
+    unsigned long long run = carry;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (j < lim) {
+        const unsigned long long v = f[j] & LB_VAL;
+        if (f[j] & LB_INC) {
+          run = v;
+        } else {
+          run += v;
+          st_relaxed(&sy.flags[F + lane * PER + j], tag | LB_INC | run);
+        }
+      }
+    }
+    // the inclusive prefix at position R-1 (held by the lane that owns it)
+    const int owner = (R - 1) / PER;
+    P = __shfl_sync(0xffffffffu, run, owner);
+    F += R;
+  }
+}
+
+// The offset scanner: one warp that turns a stream's uint16 size table into
+// the byte offset of every chunk's payload (exclusive prefix sum), tagged with
+// the launch epoch and a state bit like the lookback words.  32 entries per lane per pass, so
+// it runs far ahead of the CTAs that read the offsets.
+__device__ __forceinline__ void scan_offsets(unsigned long long* offs, unsigned int epoch, const uint16_t* table,
+                                             long long chunks) {
+  constexpr int PER = 32;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long tag = (unsigned long long)epoch << 48;
+  unsigned long long run = 0;
+  for (long long i = 0; i < chunks; i += 32 * PER) {
+    const long long b = i + (long long)lane * PER;
+    uint32_t e[PER];
+    if (b + PER <= chunks) {
+#pragma unroll
+      for (int k = 0; k < PER / 8; k++) {
+        const uint4 w = *reinterpret_cast<const uint4*>(table + b + 8 * k);
+        e[8 * k + 0] = w.x & 0xffffu; e[8 * k + 1] = w.x >> 16;
+        e[8 * k + 2] = w.y & 0xffffu; e[8 * k + 3] = w.y >> 16;
+        e[8 * k + 4] = w.z & 0xffffu; e[8 * k + 5] = w.z >> 16;
+        e[8 * k + 6] = w.w & 0xffffu; e[8 * k + 7] = w.w >> 16;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < PER; j++) e[j] = (b + j < chunks) ? table[b + j] : 0u;
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; j++) sum += e[j];
+    uint32_t total;
+    const uint32_t base = warp_scan_excl(sum, total);
+    unsigned long long o = run + base;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (b + j < chunks) offs[b + j] = tag | LB_INC | o;  // the state bit: a zeroed word is never valid
+      o += e[j];
+    }
+    run += total;
+  }
+}
+
+// Offset of chunk c's payload from the scanner's word (waits, bounded, until
+// the word carries this launch's epoch; on timeout latches the status and
+// returns 0).
+__device__ __forceinline__ unsigned long long wait_offset(const Sync& sy, unsigned int epoch, long long c) {
+  const unsigned long long t0 = globaltimer();
+  for (int it = 0;; ++it) {
+    const unsigned long long v = ld_relaxed(&sy.offs[c]);
+    if ((v >> 48) == epoch && (v & LB_INC)) return v & LB_VAL;
+    if ((it & 15) == 15) {
+      if (globaltimer() - t0 > sy.timeout_ns || *(volatile unsigned int*)sy.status != 0) {
+        latch(sy.status, DST_TIMEOUT);
+        return 0;
+      }
+      __nanosleep(128);
+    }
+  }
 }
 
 }  // namespace cortado

@@ -1,5 +1,5 @@
-// The fused per-chunk encode and decode stages and the six operations built
-// from them.  Reference counterparts:
+// The fused per-chunk encode and decode stages and the shared-memory layout
+// of the pipelined kernels built from them.  Reference counterparts:
 //   store encode   include/d_server_encode.h:51-143
 //   storage decode include/d_server_encode.h:174-260
 //   init_send      include/d_s2c.h:51-200
@@ -9,29 +9,14 @@
 // Differences in mechanism (not in output bytes): chunk offsets from a bounded,
 // epoch-tagged decoupled lookback (encoders) or a per-CTA running sum of the
 // size table (decoders); one 128-thread CTA per chunk with the data held in
-// registers; TMA for float chunks and compressed payloads; errors latched in a
-// status word instead of printf + __trap.
+// registers; TMA for float chunks and compressed payloads, prefetched one
+// chunk ahead; errors latched in a status word instead of printf + __trap.
 #pragma once
 #include "device.cuh"
 
 namespace cortado {
 
 enum Op : int { OP_STORE = 0, OP_S2C = 1, OP_RESI = 2, OP_SDEC = 3, OP_CDEC = 4, OP_RAPPLY = 5 };
-
-// Shared memory of one CTA.  buf0/buf1 are 16 KiB + slack; buf0 is 1024-byte
-// aligned for TMA's 128B swizzle.
-struct __align__(1024) Smem {
-  uint32_t buf0[CW + 64];  // float chunk (TMA), compressed payload, raw source, output staging
-  uint32_t buf1[CW + 64];  // plane buffer, then compacted output
-  uint16_t l2[NT];         // level-2 bitmap (2 bytes per segment thread)
-  uint32_t rb[NT];         // decoder: RE1 rank base per segment thread
-  uint32_t scan_a[4], scan_b[4], scan_c[4], xchg[4];
-  uint64_t bar;
-  long long chunk, next_chunk;
-  unsigned long long payload_off;
-  unsigned int epoch, is_last;
-  uint32_t info[8];
-};
 
 struct OpArgs {
   const uint8_t* in;        // store: floats; others: input stream
@@ -46,12 +31,68 @@ struct OpArgs {
   int has_map_in, has_map_out;
 };
 
-// resi_recv's third buffer (client source chunk, then output staging) follows
-// the Smem block at the next 1024-byte boundary.
-constexpr size_t SMEM_BYTES = ((sizeof(Smem) + 1023) & ~size_t(1023));
-__device__ __forceinline__ uint32_t* sm_src(Smem& sm) {
-  return reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(&sm) + SMEM_BYTES);
+// ---------------------------------------------------------------- shared memory
+// A CTA owns a 1 KiB control block followed by 2 or 3 chunk buffers of
+// BUF_WORDS words (16 KiB + slack, a multiple of 1024 bytes so that every
+// buffer keeps the 1024-byte alignment TMA's 128B swizzle needs).  Buffers 0
+// and 1 are the two pipeline stages (the chunk being processed and the one
+// being loaded); buffer 2 is the re-encoders' plane buffer or resi_recv's
+// client chunk.
+constexpr int BUF_WORDS = 4352;
+constexpr int CTL_BYTES = 1024;
+
+// What the prefetch of one queue entry found (written by warp 3, read by all
+// threads in the iteration that processes it).
+struct StageMeta {
+  long long g;              // queue index (>= the queue length: no chunk)
+  long long c;              // chunk within its stream
+  long long n;              // stream's original bytes
+  long long chunks;         // stream's chunks
+  unsigned long long off;   // decoders: payload offset in the stream's data section
+  int item;                 // batched launches: the stream
+  int nw;                   // words in the chunk
+  int tma;                  // the stage's loads complete on its mbarrier
+  int bad;                  // 1: corrupt size entry; 2: unusable stream header
+  int csize;                // decoders: payload bytes
+  int d;                    // decoders: payload's byte offset in the stage buffer
+  int tma_len;              // decoders: bytes brought by the bulk copy
+  int eb_e;                 // decoders: the stream's exponent
+};
+
+// The chunk whose payload waits in a staging buffer for its output offset
+// (written by thread 0 at the end of encode_stage, flushed one iteration later).
+struct Pend {
+  long long c;
+  int item;
+  int nw;
+  int csize;
+  int raw;
+  int valid;
+};
+
+struct __align__(16) Ctl {
+  uint16_t l2[NT];          // level-2 bitmap (2 bytes per segment thread)
+  uint16_t rb[NT];          // decoder: RE1 rank base per segment thread
+  uint32_t scan_a[4], scan_b[4], scan_c[4], xchg[4];
+  uint64_t bar[2];          // per stage: its TMA loads
+  uint64_t bar_src;         // resi_recv: the client chunk
+  StageMeta st[2];
+  Pend pend[2];             // encoders: the chunk of each stage, until it is flushed
+  unsigned long long payload_off;
+  unsigned int epoch, is_last;
+  uint32_t info[8];
+};
+static_assert(sizeof(Ctl) <= CTL_BYTES, "control block");
+
+__host__ __device__ constexpr size_t smem_bytes(int nbuf) { return CTL_BYTES + (size_t)nbuf * BUF_WORDS * 4 + 1024; }
+
+__device__ __forceinline__ uint32_t* stage_buf(Ctl& sm, int k) {
+  return reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(&sm) + CTL_BYTES + k * (BUF_WORDS * 4));
 }
+
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
 
 // Writes `csize` payload bytes to global memory at dst (any alignment) with
 // 16-byte stores for the aligned interior.  word(q) returns payload word q
@@ -99,36 +140,45 @@ __device__ __forceinline__ void plane_offsets(int tid, uint32_t& e, uint32_t& o)
 
 // ============================================================== encode stage
 // Input: v[32] = the pre-DIFFMS words of group g = threadIdx.x (quantized bins
-// or residuals; words at or beyond nw are 0), the raw source (those words in a
-// swizzled buffer, used when the chunk does not compress).  Produces the
-// chunk's payload in the output stream and its size-table entry
-// (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1 -> raw fallback -> carry -> s2g).
+// or residuals; words at or beyond nw are 0).  `plane` is a swizzled 16 KiB
+// buffer that may be overwritten once every thread has passed the first
+// barrier; it becomes the plane buffer and then the staging of the compacted
+// payload (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1, raw fallback).  The chunk's size
+// is published for the lookback; the payload is written out later by
+// flush_chunk, once the size of every earlier chunk is known.  raw_copy, when
+// not null, is a swizzled buffer holding the pre-DIFFMS words, copied (linear)
+// into the staging buffer when the chunk does not compress; otherwise a raw
+// chunk's words are read back from the input by the flush.  The chunk is
+// recorded in `pend`.  after_publish() runs on every thread once the size is
+// published (it may hold barriers: the pipelined loops flush the previous
+// chunk there, a whole iteration after that chunk's own publication).
 // FULL: a whole 16 KiB chunk (nw == 4096), with compile-time addressing.
-template <bool FULL>
-__device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t (&v)[32], const uint32_t* raw_src,
-                                             long long c, int nw_in, long long chunks, uint8_t* data_out,
-                                             uint16_t* table_out) {
+template <bool FULL, typename Hook>
+__device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (&v)[32], uint32_t* plane,
+                                             const uint32_t* raw_copy, long long c, int nw_in, int item,
+                                             Pend& pend, Hook after_publish) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = FULL ? CW : nw_in;
   const int osize = nw * 4;
   const int G = nw >> 5, rem = nw & 31;
+  uint8_t* st = reinterpret_cast<uint8_t*>(plane);
 
   // DIFFMS (d_DIFFMS.h:44-66): word minus its predecessor, then zig-zag.
   if (lane == 31) sm.xchg[warp] = v[31];
   uint32_t vany = 0;
 #pragma unroll
   for (int k = 0; k < 32; k++) vany |= v[k];
-  if (!__syncthreads_or(vany != 0)) {
+  const bool any_nz = __syncthreads_or(vany != 0);
+  if (!any_nz) {
     // All words zero: DIFFMS, BIT_4 and zero elimination leave no byte, so
     // RZE_1 emits only its 2-byte trailer (the original chunk size).
-    if (warp == 0) {
-      const unsigned long long X = lookback(a.sy, sm.epoch, c, 2u);
-      if (lane < 2) data_out[X + lane] = (uint8_t)(osize >> (8 * lane));
-      if (lane == 0) {
-        table_out[c] = 2;
-        if (c == chunks - 1) *a.out_size = HDR + 2 * chunks + (long long)(X + 2);
-      }
+    if (tid == 0) {
+      lookback_publish(sy, sm.epoch, c, 2u);
+      st[0] = (uint8_t)osize;
+      st[1] = (uint8_t)(osize >> 8);
+      pend = Pend{c, item, nw, 2, 0, 1};
     }
+    after_publish();
     return;
   }
   uint32_t prev = __shfl_up_sync(0xffffffffu, v[31], 1);
@@ -147,7 +197,6 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   }
   // BIT_4: full groups are transposed into the planes (plane s at linear
   // words s*G .. s*G+G-1); the trailing partial group is copied untransposed.
-  uint32_t* plane = sm.buf1;
   if (FULL) {
     uint32_t any = 0;
 #pragma unroll
@@ -214,57 +263,55 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
   const uint32_t NZ = tot & 0xffffu, C1 = tot >> 16;
   const uint32_t zoff = ex & 0xffffu, c1off = ex >> 16;
   // (barrier inside the scan: the plane buffer is now free -> staging)
-  uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf1);
 
-  unsigned int w0_csize = 0;
-  if (warp == 0) {
-    // Levels 2 and 3 and the top bitmap (d_REencode1wordperthread), one warp.
-    const uint2 b2 = reinterpret_cast<const uint2*>(sm.l2)[lane];
-    const uint32_t pprev = __shfl_up_sync(0xffffffffu, b2.y >> 24, 1);
-    const uint32_t p0 = lane ? pprev : 0u;
-    const uint32_t k2 = nz_nibble(b2.x ^ ((b2.x << 8) | p0)) | (nz_nibble(b2.y ^ ((b2.y << 8) | (b2.x >> 24))) << 4);
-    uint32_t C2;
-    const uint32_t off2 = warp_scan_excl(__popc(k2), C2);
-    const uint32_t p3 = __shfl_up_sync(0xffffffffu, k2, 1);
-    const bool keep3 = k2 != (lane ? p3 : 0u);
-    const uint32_t top = __ballot_sync(0xffffffffu, keep3);
-    const uint32_t C3 = __popc(top);
-    const uint32_t off3 = __popc(top & ((1u << lane) - 1u));
-    const uint32_t T = NZ + C1 + C2 + C3;
-    unsigned int csize = (NZ == 0) ? 2u : T + 6u;
-    const bool raw = csize >= (unsigned)osize;
-    if (raw) csize = osize;
-    // Publish now, wait for the predecessors' prefix after the compaction.
-    if (lane == 0) {
-      lookback_publish(a.sy, sm.epoch, c, csize);
-      sm.info[0] = csize;
-      sm.info[1] = raw;
+  // Levels 2 and 3 and the top bitmap (d_REencode1wordperthread) from the
+  // 256-byte level-2 bitmap; every warp derives the chunk size, so no barrier
+  // is needed before the compaction; warp 0 writes the bytes.
+  const uint2 b2 = reinterpret_cast<const uint2*>(sm.l2)[lane];
+  const uint32_t pprev = __shfl_up_sync(0xffffffffu, b2.y >> 24, 1);
+  const uint32_t p0 = lane ? pprev : 0u;
+  const uint32_t k2 = nz_nibble(b2.x ^ ((b2.x << 8) | p0)) | (nz_nibble(b2.y ^ ((b2.y << 8) | (b2.x >> 24))) << 4);
+  uint32_t C2;
+  const uint32_t off2 = warp_scan_excl(__popc(k2), C2);
+  const uint32_t p3 = __shfl_up_sync(0xffffffffu, k2, 1);
+  const bool keep3 = k2 != (lane ? p3 : 0u);
+  const uint32_t top = __ballot_sync(0xffffffffu, keep3);
+  const uint32_t C3 = __popc(top);
+  const uint32_t off3 = __popc(top & ((1u << lane) - 1u));
+  const uint32_t T = NZ + C1 + C2 + C3;
+  unsigned int csize = (NZ == 0) ? 2u : T + 6u;
+  const bool raw = csize >= (unsigned)osize;
+  if (raw) csize = osize;
+  if (tid == 0) {
+    lookback_publish(sy, sm.epoch, c, csize);
+    pend = Pend{c, item, nw, (int)csize, (int)raw, 1};
+  }
+  after_publish();
+  if (raw) {
+    if (raw_copy) {
+      for (int w = tid; w < nw; w += NT) plane[w] = raw_copy[swz(w)];
     }
-    w0_csize = csize;
-    if (!raw) {
-      if (NZ == 0) {
-        if (lane == 0) {
-          st[0] = (uint8_t)osize;
-          st[1] = (uint8_t)(osize >> 8);
-        }
-      } else {
-        uint32_t p = NZ + C1 + off2;
-#pragma unroll
-        for (int j = 0; j < 8; j++)
-          if ((k2 >> j) & 1) st[p++] = (uint8_t)((j < 4 ? b2.x : b2.y) >> (8 * (j & 3)));
-        if (keep3) st[NZ + C1 + C2 + off3] = (uint8_t)k2;
-        if (lane < 4) st[T + lane] = (uint8_t)(top >> (8 * lane));
-        if (lane == 4) st[T + 4] = (uint8_t)osize;
-        if (lane == 5) st[T + 5] = (uint8_t)(osize >> 8);
+    return;
+  }
+  if (warp == 0) {
+    if (NZ == 0) {
+      if (lane == 0) {
+        st[0] = (uint8_t)osize;
+        st[1] = (uint8_t)(osize >> 8);
       }
+    } else {
+      uint32_t p = NZ + C1 + off2;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if ((k2 >> j) & 1) st[p++] = (uint8_t)((j < 4 ? b2.x : b2.y) >> (8 * (j & 3)));
+      if (keep3) st[NZ + C1 + C2 + off3] = (uint8_t)k2;
+      if (lane < 4) st[T + lane] = (uint8_t)(top >> (8 * lane));
+      if (lane == 4) st[T + 4] = (uint8_t)osize;
+      if (lane == 5) st[T + 5] = (uint8_t)(osize >> 8);
     }
   }
-  // Compaction of the zero-eliminated bytes and the kept level-1 bitmap bytes
-  // (all warps; the result is discarded if warp 0 decides the chunk is raw).
-  // Skipped when ZE + RE1 alone already reach the chunk size: the chunk is
-  // then certainly raw, and the writes could run past the staging buffer.
-  const bool fits = NZ + C1 + 6 < (uint32_t)osize;
-  if (nz && fits) {
+  // Compaction of the zero-eliminated bytes and the kept level-1 bitmap bytes.
+  if (nz) {
     uint32_t p = zoff;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
@@ -282,132 +329,83 @@ __device__ __forceinline__ void encode_chunk(Smem& sm, const OpArgs& a, uint32_t
       }
     }
   }
-  if (K && fits) {
+  if (K) {
     uint32_t p = NZ + c1off;
 #pragma unroll
     for (int j = 0; j < 16; j++)
       if ((K >> j) & 1) st[p++] = (uint8_t)(M[j >> 2] >> (8 * (j & 3)));
   }
-  if (warp == 0) {
-    const unsigned long long X = lookback_published(a.sy, sm.epoch, c, w0_csize);
-    if (lane == 0) sm.payload_off = X;
-  }
-  __syncthreads();
-  const unsigned int csize = sm.info[0];
-  const bool raw = sm.info[1];
+}
+
+// Writes out a pending chunk (p, output offset sm.payload_off, both visible
+// after a barrier) from its staging buffer -- or, for a raw chunk without a
+// staged copy, from raw_word(w) -- and its size-table entry; the stream's last
+// chunk also sets the stream size.
+template <typename RawWord>
+__device__ __forceinline__ void flush_chunk(const Ctl& sm, const Pend& p, const uint32_t* staging, bool raw_staged,
+                                            RawWord raw_word, uint8_t* data_out, uint16_t* table_out,
+                                            long long* out_size, long long chunks) {
   const unsigned long long X = sm.payload_off;
-  if (raw) {
-    store_payload(data_out + X, csize, [&](int w) -> uint32_t { return w < nw ? raw_src[swz(w)] : 0u; });
+  const int nw = p.nw;
+  if (p.raw && !raw_staged) {
+    store_payload(data_out + X, p.csize, [&](int w) -> uint32_t { return w < nw ? raw_word(w) : 0u; });
   } else {
-    store_payload(data_out + X, csize, [&](int w) -> uint32_t { return sm.buf1[w]; });
+    store_payload(data_out + X, p.csize, [&](int w) -> uint32_t { return staging[w]; });
   }
-  if (tid == 0) {
-    table_out[c] = (uint16_t)csize;
-    if (c == chunks - 1) *a.out_size = HDR + 2 * chunks + (long long)(X + csize);
+  if (threadIdx.x == 0) {
+    table_out[p.c] = (uint16_t)p.csize;
+    if (p.c == chunks - 1) *out_size = HDR + 2 * chunks + (long long)(X + p.csize);
   }
 }
 
 // ============================================================== decode stage
-// Finds chunk c's payload (running sum of the size table, as the reference's
-// decoders do, d_s2c.h:98-106), loads it with a TMA bulk copy, undoes RZE_1,
-// BIT_4 and DIFFMS, and returns the pre-pipeline words of group
-// g = threadIdx.x in v[32] (words at or beyond nw are 0).  *raw reports a chunk
-// stored uncompressed (its words are returned as stored).
-struct DecState {
-  long long prev_c;
-  unsigned long long prev_off;
-  uint32_t phase;
-};
-
-template <bool FULL>
-__device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw_in,
-                                             long long chunks, const uint16_t* table, const uint8_t* data_in,
-                                             long long data_bytes, uint32_t (&v)[32], bool& raw_out,
-                                             const CUtensorMap* src_map, int src_row) {
-  const bool also_src = src_map != nullptr;
+// Undoes RZE_1, BIT_4 and DIFFMS for the chunk whose payload the stage's
+// loads brought into P (at byte offset m.d, m.csize bytes; see StageMeta) and
+// returns the pre-pipeline words of group g = threadIdx.x in v[32] (words at
+// or beyond nw are 0).  raw_out reports a chunk stored uncompressed (its words
+// are returned as stored).  `plane` is the swizzled buffer for the BIT_4
+// planes; when it is P itself the payload is expanded into registers first
+// (one more barrier) and P ends up holding the planes.  side() runs on every
+// thread before the first barrier: warp 3 prefetches the next chunk there
+// while warp 0 decodes this chunk's bitmaps.
+template <bool FULL, typename Side>
+__device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const StageMeta& m, uint32_t* P,
+                                            uint32_t* plane, uint32_t (&v)[32], bool& raw_out, Side side) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nw = FULL ? CW : nw_in;
+  const int nw = FULL ? CW : m.nw;
   const int osize = nw * 4;
   const int G = nw >> 5, rem = nw & 31;
-  uint8_t* st = reinterpret_cast<uint8_t*>(sm.buf0);
-
-  // Payload offset: warp 0 sums the size-table entries since its last chunk
-  // (8 entries per 16-byte load; the ragged ends entry by entry).
-  if (warp == 0) {
-    unsigned long long s = 0;
-    const long long lo = ds.prev_c, hi = c;
-    const long long vlo = (lo + 7) & ~7LL, vhi = hi & ~7LL;  // 16-byte-aligned entries of the table
-    if (vlo < vhi) {
-      const uint4* t4 = reinterpret_cast<const uint4*>(table);
-      for (long long i = vlo / 8 + lane; i < vhi / 8; i += 32) {
-        const uint4 w = t4[i];
-        s += (w.x & 0xffffu) + (w.x >> 16) + (w.y & 0xffffu) + (w.y >> 16) + (w.z & 0xffffu) + (w.z >> 16) +
-             (w.w & 0xffffu) + (w.w >> 16);
-      }
-      for (long long i = lo + lane; i < vlo; i += 32) s += table[i];
-      for (long long i = vhi + lane; i < hi; i += 32) s += table[i];
-    } else {
-      for (long long i = lo + lane; i < hi; i += 32) s += table[i];
-    }
-    s = warp_sum64(s);
-    ds.prev_off += s;
-    ds.prev_c = c;
-    if (lane == 0) {
-      const int cs = table[c];
-      const long long off = (long long)ds.prev_off;
-      int bad = (cs > osize) || (cs < 2 && cs != osize) || (off + cs > data_bytes);
-      sm.info[0] = bad ? 0u : (uint32_t)cs;
-      sm.info[1] = bad;
-      sm.payload_off = off;
-      // TMA: 16-byte-aligned interior of the payload; the ragged tail by hand.
-      const uintptr_t A = reinterpret_cast<uintptr_t>(data_in + off);
-      const uintptr_t a0 = A & ~uintptr_t(15);
-      uintptr_t a1 = (A + (bad ? 0 : cs)) & ~uintptr_t(15);
-      if (a1 < a0) a1 = a0;
-      sm.info[2] = (uint32_t)(A - a0);
-      sm.info[3] = (uint32_t)(a1 - a0);
-      uint32_t tx = (uint32_t)(a1 - a0) + (also_src ? (uint32_t)CS : 0u);
-      bulk_wait_read();  // a previous TMA store may still be reading buf0
-      fence_proxy_async();
-      if (tx) {
-        mbar_expect_tx(&sm.bar, tx);
-        if (a1 > a0) bulk_load(st, reinterpret_cast<const void*>(a0), (uint32_t)(a1 - a0), &sm.bar);
-        if (also_src) tma_load_rows(sm_src(sm), src_map, src_row, &sm.bar);
-      }
-      sm.info[4] = tx != 0;
-    }
-  }
-  __syncthreads();
-  const int csize = (int)sm.info[0];
-  const int d = (int)sm.info[2];
-  const int tma_len = (int)sm.info[3];
-  {
-    const uint8_t* g = data_in + sm.payload_off;
-    const int from = tma_len - d;  // payload bytes [from, csize) are loaded by hand
-    for (int i = tid + (from > 0 ? from : 0); i < csize; i += NT) st[d + i] = g[i];
-  }
-  if (sm.info[4]) {
-    if (!mbar_wait(&sm.bar, ds.phase, a.sy.timeout_ns)) latch(a.sy.status, DST_TIMEOUT);
-    ds.phase ^= 1;
-  }
-  __syncthreads();
+  const bool inplace = plane == P;
+  const uint8_t* st = reinterpret_cast<const uint8_t*>(P);
+  const int csize = m.csize;
+  const int d = m.d;
+  side();
   raw_out = false;
-  if (sm.info[1]) {  // corrupt size entry
-    if (tid == 0) latch(a.sy.status, DST_CORRUPT);
+  if (m.bad) {  // corrupt size entry or stream header
+    if (tid == 0) latch(sy.status, m.bad == 1 ? DST_CORRUPT : DST_SIZE_MISMATCH);
 #pragma unroll
     for (int k = 0; k < 32; k++) v[k] = 0;
+    __syncthreads();
     return;
   }
   if (csize == osize) {
-    // Stored uncompressed: realign the payload words into the plane buffer.
+    // Stored uncompressed: realign the payload words (thread t: words
+    // t + 128j, conflict-free) into the swizzled plane buffer.
     raw_out = true;
-    for (int w = tid; w < nw; w += NT) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const int w = tid + NT * j;
       const int o = d + 4 * w;
-      const uint32_t lo = sm.buf0[o >> 2], hi = sm.buf0[(o >> 2) + 1];
-      sm.buf1[swz(w)] = __funnelshift_r(lo, hi, 8 * (o & 3));
+      v[j] = (FULL || w < nw) ? __funnelshift_r(P[o >> 2], P[(o >> 2) + 1], 8 * (o & 3)) : 0u;
+    }
+    if (inplace) __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const int w = tid + NT * j;
+      if (FULL || w < nw) plane[swz(w)] = v[j];
     }
     __syncthreads();
-    row_load(sm.buf1, tid, v);
+    row_load(plane, tid, v);
     if (!FULL && 32 * tid + 32 > nw) {
 #pragma unroll
       for (int k = 0; k < 32; k++)
@@ -416,78 +414,72 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     return;
   }
   // ---- undo RZE_1 (d_iRZE, d_RZE.h:127-206)
-  bool ok = true;
   const int orig = st[d + csize - 2] | (st[d + csize - 1] << 8);
-  ok = (orig == osize);
+  bool ok = (orig == osize);
   if (csize == 2) {
     // Trailer only: the BIT_4 output was all zero, so every word decodes to 0.
-    if (!ok && tid == 0) latch(a.sy.status, DST_CORRUPT);
+    if (!ok && tid == 0) latch(sy.status, DST_CORRUPT);
 #pragma unroll
     for (int k = 0; k < 32; k++) v[k] = 0;
-    __syncthreads();  // the trailer was read from buf0, which the caller reuses
+    __syncthreads();  // the trailer was read from P, which the caller reuses
     return;
   }
   uint32_t M[4] = {0, 0, 0, 0};
-  uint32_t zbase = 0;
-  if (csize == 2) {
-    // all-zero BIT_4 output
-  } else {
-    const int T = csize - 6;
-    if (warp == 0) {
-      bool wok = T >= 0;
-      const int Tc = T < 0 ? 0 : T;
-      const uint32_t top = (uint32_t)st[d + Tc] | ((uint32_t)st[d + Tc + 1] << 8) | ((uint32_t)st[d + Tc + 2] << 16) |
-                           ((uint32_t)st[d + Tc + 3] << 24);
-      const int c3 = __popc(top);
-      wok = wok && (c3 <= T);
-      const int b3 = Tc - c3;
-      const int r3 = __popc(top & (0xffffffffu >> (31 - lane))) - 1;
-      const uint32_t l3 = (r3 >= 0 && wok) ? st[d + b3 + r3] : 0u;
-      uint32_t c2u;
-      const uint32_t e2 = warp_scan_excl(__popc(l3), c2u);
-      const int c2 = (int)c2u;
-      wok = wok && (c3 + c2 <= T);
-      const int b2 = b3 - c2;
-      uint32_t l2lo = 0, l2hi = 0;
-      uint8_t prevb = 0;
-      if (wok && e2 > 0) prevb = st[d + b2 + e2 - 1];
-      uint32_t rk = e2;
+  const int T = csize - 6;
+  if (warp == 0) {
+    bool wok = T >= 0;
+    const int Tc = T < 0 ? 0 : T;
+    const uint32_t top = (uint32_t)st[d + Tc] | ((uint32_t)st[d + Tc + 1] << 8) | ((uint32_t)st[d + Tc + 2] << 16) |
+                         ((uint32_t)st[d + Tc + 3] << 24);
+    const int c3 = __popc(top);
+    wok = wok && (c3 <= T);
+    const int b3 = Tc - c3;
+    const int r3 = __popc(top & (0xffffffffu >> (31 - lane))) - 1;
+    const uint32_t l3 = (r3 >= 0 && wok) ? st[d + b3 + r3] : 0u;
+    uint32_t c2u;
+    const uint32_t e2 = warp_scan_excl(__popc(l3), c2u);
+    const int c2 = (int)c2u;
+    wok = wok && (c3 + c2 <= T);
+    const int b2 = b3 - c2;
+    uint32_t l2lo = 0, l2hi = 0;
+    uint8_t prevb = 0;
+    if (wok && e2 > 0) prevb = st[d + b2 + e2 - 1];
+    uint32_t rk = e2;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        if ((l3 >> j) & 1) prevb = wok ? st[d + b2 + rk++] : 0;
-        if (j < 4) l2lo |= (uint32_t)prevb << (8 * j);
-        else l2hi |= (uint32_t)prevb << (8 * (j - 4));
-      }
-      reinterpret_cast<uint2*>(sm.l2)[lane] = make_uint2(l2lo, l2hi);
-      // RE1 rank base for segment threads 4*lane .. 4*lane+3.
-      const uint32_t p0 = __popc(l2lo & 0xffffu), p1 = __popc(l2lo >> 16), p2 = __popc(l2hi & 0xffffu);
-      const uint32_t p3 = __popc(l2hi >> 16);
-      uint32_t c1u;
-      const uint32_t e1 = warp_scan_excl(p0 + p1 + p2 + p3, c1u);
-      sm.rb[4 * lane] = e1;
-      sm.rb[4 * lane + 1] = e1 + p0;
-      sm.rb[4 * lane + 2] = e1 + p0 + p1;
-      sm.rb[4 * lane + 3] = e1 + p0 + p1 + p2;
-      const int c1 = (int)c1u;
-      wok = wok && (c3 + c2 + c1 <= T);
-      if (lane == 0) {
-        sm.info[5] = wok ? (uint32_t)(b2 - c1) : 0u;  // start of RE1 data = count of ZE bytes
-        sm.info[6] = wok;
-      }
+    for (int j = 0; j < 8; j++) {
+      if ((l3 >> j) & 1) prevb = wok ? st[d + b2 + rk++] : 0;
+      if (j < 4) l2lo |= (uint32_t)prevb << (8 * j);
+      else l2hi |= (uint32_t)prevb << (8 * (j - 4));
     }
-    __syncthreads();
-    const bool wok = sm.info[6];
-    ok = ok && wok;
-    zbase = sm.info[5];
-    if (wok) {
-      const uint32_t Kb = sm.l2[tid];
-      uint32_t rk = sm.rb[tid];
-      uint8_t prevb = rk > 0 ? st[d + zbase + rk - 1] : 0;
+    reinterpret_cast<uint2*>(sm.l2)[lane] = make_uint2(l2lo, l2hi);
+    // RE1 rank base for segment threads 4*lane .. 4*lane+3.
+    const uint32_t p0 = __popc(l2lo & 0xffffu), p1 = __popc(l2lo >> 16), p2 = __popc(l2hi & 0xffffu);
+    const uint32_t p3 = __popc(l2hi >> 16);
+    uint32_t c1u;
+    const uint32_t e1 = warp_scan_excl(p0 + p1 + p2 + p3, c1u);
+    sm.rb[4 * lane] = (uint16_t)e1;
+    sm.rb[4 * lane + 1] = (uint16_t)(e1 + p0);
+    sm.rb[4 * lane + 2] = (uint16_t)(e1 + p0 + p1);
+    sm.rb[4 * lane + 3] = (uint16_t)(e1 + p0 + p1 + p2);
+    const int c1 = (int)c1u;
+    wok = wok && (c3 + c2 + c1 <= T);
+    if (lane == 0) {
+      sm.info[5] = wok ? (uint32_t)(b2 - c1) : 0u;  // start of RE1 data = count of ZE bytes
+      sm.info[6] = wok;
+    }
+  }
+  __syncthreads();
+  const bool wok = sm.info[6];
+  ok = ok && wok;
+  const uint32_t zbase = sm.info[5];
+  if (wok) {
+    const uint32_t Kb = sm.l2[tid];
+    uint32_t rk = sm.rb[tid];
+    uint8_t prevb = rk > 0 ? st[d + zbase + rk - 1] : 0;
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        if ((Kb >> j) & 1) prevb = st[d + zbase + rk++];
-        M[j >> 2] |= (uint32_t)prevb << (8 * (j & 3));
-      }
+    for (int j = 0; j < 16; j++) {
+      if ((Kb >> j) & 1) prevb = st[d + zbase + rk++];
+      M[j >> 2] |= (uint32_t)prevb << (8 * (j & 3));
     }
   }
   // bitmap bits beyond the chunk must be clear
@@ -503,9 +495,8 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   const uint32_t nz = __popc(M[0]) + __popc(M[1]) + __popc(M[2]) + __popc(M[3]);
   uint32_t NZ;
   const uint32_t zoff = block_scan_excl(nz, sm.scan_b, NZ);
-  if (csize != 2 && NZ != zbase) ok = false;
-  if (csize == 2 && NZ != 0) ok = false;
-  if (!ok) latch(a.sy.status, DST_CORRUPT);
+  if (NZ != zbase) ok = false;
+  if (!ok) latch(sy.status, DST_CORRUPT);
   // ZE decode: scatter the non-zero bytes back into the 32 words.
   uint32_t q[32];
   if (!ok || (M[0] | M[1] | M[2] | M[3]) == 0) {
@@ -515,17 +506,18 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     uint32_t p = (uint32_t)d + zoff;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
-      const uint32_t m = (M[k >> 3] >> (4 * (k & 7))) & 15u;
+      const uint32_t mk = (M[k >> 3] >> (4 * (k & 7))) & 15u;
       uint32_t x = 0;
-      if (m) {
-        const uint32_t lo = sm.buf0[p >> 2], hi = sm.buf0[(p >> 2) + 1];
-        x = __byte_perm(__funnelshift_r(lo, hi, 8 * (p & 3)), 0u, expand_sel(m));
-        p += __popc(m);
+      if (mk) {
+        const uint32_t lo = P[p >> 2], hi = P[(p >> 2) + 1];
+        x = __byte_perm(__funnelshift_r(lo, hi, 8 * (p & 3)), 0u, expand_sel(mk));
+        p += __popc(mk);
       }
       q[k] = x;
     }
   }
-  row_store(sm.buf1, tid, q);
+  if (inplace) __syncthreads();  // every payload byte has been read
+  row_store(plane, tid, q);
   __syncthreads();
   // ---- undo BIT_4 (d_iBIT_4): gather plane words of group g, transpose.
   if (FULL) {
@@ -534,17 +526,17 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     uint32_t any = 0;
 #pragma unroll
     for (int s = 0; s < 32; s++) {
-      v[s] = sm.buf1[128 * s + ((s & 1) ? po : pe)];
+      v[s] = plane[128 * s + ((s & 1) ? po : pe)];
       any |= v[s];
     }
     if (any) transpose32(v);
   } else if (tid < G) {
 #pragma unroll
-    for (int s = 0; s < 32; s++) v[s] = sm.buf1[swz(s * G + tid)];
+    for (int s = 0; s < 32; s++) v[s] = plane[swz(s * G + tid)];
     transpose32(v);
   } else {
 #pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = (tid == G && k < rem) ? sm.buf1[swz(32 * G + k)] : 0u;
+    for (int k = 0; k < 32; k++) v[k] = (tid == G && k < rem) ? plane[swz(32 * G + k)] : 0u;
   }
   // ---- undo DIFFMS (d_iDIFFMS, d_DIFFMS.h:69-102): un-zig-zag, prefix sum.
   uint32_t acc = 0;
@@ -555,7 +547,7 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
     v[k] = acc;
   }
   uint32_t dummy;
-  const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);
+  const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);  // (its barrier: every plane read is done)
 #pragma unroll
   for (int k = 0; k < 32; k++) v[k] += carry;
   if (!FULL && 32 * tid + 32 > nw) {
@@ -565,24 +557,23 @@ __device__ __forceinline__ void decode_chunk(Smem& sm, const OpArgs& a, DecState
   }
 }
 
-// The partial last chunk of a stream (at most one per launch) runs out of
+// The partial last chunk of a stream (at most one per stream) runs out of
 // line, so the full-chunk loop body stays small enough for the instruction
 // caches.  Arrays pass through local memory on this rare path.
-__device__ __noinline__ void encode_chunk_partial(Smem& sm, const OpArgs& a, uint32_t* v, const uint32_t* raw_src,
-                                                  long long c, int nw, long long chunks, uint8_t* data_out,
-                                                  uint16_t* table_out) {
+__device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint32_t* v, uint32_t* plane,
+                                                  const uint32_t* raw_copy, long long c, int nw, int item,
+                                                  Pend& pend) {
   uint32_t w[32];
 #pragma unroll
   for (int k = 0; k < 32; k++) w[k] = v[k];
-  encode_chunk<false>(sm, a, w, raw_src, c, nw, chunks, data_out, table_out);
+  encode_stage<false>(sm, sy, w, plane, raw_copy, c, nw, item, pend, NoHook{});
 }
 
-__device__ __noinline__ void decode_chunk_partial(Smem& sm, const OpArgs& a, DecState& ds, long long c, int nw,
-                                                  long long chunks, const uint16_t* table, const uint8_t* data_in,
-                                                  long long data_bytes, uint32_t* v, bool& raw_out,
-                                                  const CUtensorMap* src_map, int src_row) {
+template <typename Side>
+__device__ __noinline__ void decode_core_partial(Ctl& sm, const Sync& sy, const StageMeta& m, uint32_t* P,
+                                                 uint32_t* plane, uint32_t* v, bool& raw_out, Side side) {
   uint32_t w[32];
-  decode_chunk<false>(sm, a, ds, c, nw, chunks, table, data_in, data_bytes, w, raw_out, src_map, src_row);
+  decode_core<false>(sm, sy, m, P, plane, w, raw_out, side);
 #pragma unroll
   for (int k = 0; k < 32; k++) v[k] = w[k];
 }
