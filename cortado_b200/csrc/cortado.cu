@@ -357,12 +357,13 @@ __device__ __forceinline__ void prefetch_stream(Ctl& sm, int t, long long g, con
 // lookback word into an inclusive prefix, so no CTA waits on its
 // predecessors while it holds the SM.
 
-// Resolves and writes out the chunk pending in stage t (if any): warp 0 finds
-// its output offset, a barrier publishes it, every thread stores the payload.
+// Resolves and writes out the chunk pending in slot t (if any): warp 0 finds
+// its output offset, a barrier publishes it, every thread stores the payload
+// from `staging`, or a raw chunk's words from raw_word(args, chunk, w).
 // Called by every thread.
-template <class Src, typename RawWordOf>
-__device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, const uint32_t* staging, bool raw_staged,
-                                              RawWordOf raw_word_of) {
+template <class Src, typename RawWord>
+__device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, const uint8_t* staging,
+                                              RawWord raw_word) {
   Pend& pd = sm.pend[t];
   const bool valid = pd.valid;  // written before an earlier barrier
   if (valid && threadIdx.x < 32) {
@@ -373,15 +374,18 @@ __device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, co
   if (valid) {
     const OpArgs& Q = src.args(pd.item);
     const long long chunks = (Q.n + CS - 1) / CS;
-    flush_chunk(sm, pd, staging, raw_staged, raw_word_of(Q, pd.c), Q.out + HDR + 2 * chunks,
+    const long long c = pd.c;
+    flush_chunk(sm, pd, reinterpret_cast<const uint32_t*>(staging), false,
+                [&](int w) -> uint32_t { return raw_word(Q, c, w); }, Q.out + HDR + 2 * chunks,
                 reinterpret_cast<uint16_t*>(Q.out + HDR), Q.out_size, chunks);
   }
 }
 
 // store (d_server_encode_kernel): floats -> SQ -> encode.  A chunk arrives in
-// stage buffer s, becomes its plane buffer and then its staging; the previous
-// chunk's staging (buffer s^1) is flushed once this chunk's size is
-// published, and the next chunk is then loaded into buffer s^1.
+// buffer 0, which becomes its plane buffer; its compacted payload goes to
+// buffer 1 once the previous chunk's payload has been flushed from there (that
+// flush runs as soon as this chunk's size is published).  The next chunk is
+// loaded when the compaction has read buffer 0.
 template <class Src>
 __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -392,61 +396,63 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
   }
   WalkState ws{-1};
   __syncthreads();
+  uint32_t* A = stage_buf(sm, 0);
+  uint8_t* B = reinterpret_cast<uint8_t*>(stage_buf(sm, 1));
   // a raw chunk stores the original floats, read again from global memory
-  auto raw_word_of = [](const OpArgs& Q, long long c) {
-    const uint32_t* gin = reinterpret_cast<const uint32_t*>(Q.in) + c * (long long)CW;
-    return [gin](int w) -> uint32_t { return gin[w]; };
+  auto raw_word = [](const OpArgs& Q, long long c, int w) -> uint32_t {
+    return reinterpret_cast<const uint32_t*>(Q.in)[c * (long long)CW + w];
   };
-  auto take_next = [&](int t) {
+  auto take_next = [&]() {
     if (warp == 3) {
       long long g = 0;
       if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
-      prefetch_floats(sm, t, __shfl_sync(0xffffffffu, g, 0), src, ws);
+      prefetch_floats(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
     }
   };
-  take_next(0);
-  uint32_t phase = 0;  // bit s: parity of stage s's barrier
-  int s = 0;
+  take_next();
+  uint32_t phase = 0;
+  int s = 0;  // pending-chunk slot of this iteration's chunk
   for (;; s ^= 1) {
-    if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
-    phase ^= 1u << s;
-    const StageMeta& m = sm.st[s];
+    if (!mbar_wait(&sm.bar[0], phase & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u;
+    const StageMeta& m = sm.st[0];
     if (m.g >= src.total) break;
     const int item = m.item;
-    const OpArgs& A = src.args(item);
+    const OpArgs& A_ = src.args(item);
     const long long c = m.c;
     const int nw = m.nw;
-    uint32_t* buf = stage_buf(sm, s);
     if (!m.tma) {
-      load_plain_rows(buf, A.in, c, nw);
+      load_plain_rows(A, A_.in, c, nw);
       __syncthreads();
     }
-    if (Src::batched && c == 0 && tid == 0) write_header(A.out, A.n, A.q1.eb_e);
+    if (Src::batched && c == 0 && tid == 0) write_header(A_.out, A_.n, A_.q1.eb_e);
     uint32_t v[32];
-    row_load(buf, tid, v);
-    const Quant q1 = A.q1;
+    row_load(A, tid, v);
+    const Quant q1 = A_.q1;
 #pragma unroll
     for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], q1);
-    uint32_t* prev_buf = stage_buf(sm, s ^ 1);
-    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, prev_buf, false, raw_word_of); };
+    auto flush_prev = [&]() {
+      flush_pending(sm, src, s ^ 1, B, raw_word);
+      __syncthreads();  // buffer 1 has been read
+    };
     if (nw == CW) {
-      encode_stage<true>(sm, A.sy, v, buf, nullptr, c, nw, item, sm.pend[s], flush_prev);
+      encode_stage<true>(sm, A_.sy, v, A, B, c, nw, item, sm.pend[s], flush_prev);
     } else {
-      encode_stage_partial(sm, A.sy, v, buf, nullptr, c, nw, item, sm.pend[s]);
       flush_prev();
+      encode_stage_partial(sm, A_.sy, v, A, B, c, nw, item, sm.pend[s]);
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
-    __syncthreads();  // buffer s^1 has been flushed and can take the next chunk
-    take_next(s ^ 1);
+    __syncthreads();  // buffer 0 has been read
+    take_next();
   }
-  flush_pending(sm, src, s ^ 1, stage_buf(sm, s ^ 1), false, raw_word_of);
+  flush_pending(sm, src, s ^ 1, B, raw_word);
 }
 
 // init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
 // decode the stored chunk, requantize or form the residual, encode.  The
-// payload arrives in buffer 0 (which then holds the requantized words for the
-// raw fallback); buffers 1 and 2 alternate as the plane buffer of both halves
-// and the staging that waits for the flush.
+// payload of the chunk in stage s arrives in buffer s, which then holds the
+// requantized words (the raw fallback) and finally the compacted payload until
+// the next iteration flushes it; buffer 2 is the plane buffer of both halves.
 template <int OP, class Src>
 __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -459,30 +465,31 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
   __syncthreads();  // sm.epoch
   if (gridDim.x == 1 && warp == 1) src.scan(sm.epoch);
   __syncthreads();
-  auto raw_word_of = [](const OpArgs&, long long) { return [](int) -> uint32_t { return 0u; }; };
-  auto take_next = [&]() {
+  auto take_next = [&](int t) {
     if (warp == 3) {
       long long g = 0;
       if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
-      prefetch_stream(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
+      prefetch_stream(sm, t, __shfl_sync(0xffffffffu, g, 0), src, ws);
     }
   };
-  take_next();
-  uint32_t* P = stage_buf(sm, 0);
+  take_next(0);
+  uint32_t* C = stage_buf(sm, 2);
   uint32_t phase = 0;
   int s = 0;
   for (;; s ^= 1) {
-    uint32_t* C = stage_buf(sm, 1 + s);
-    uint32_t* Cprev = stage_buf(sm, 2 - s);
-    if (!mbar_wait(&sm.bar[0], phase & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
-    phase ^= 1u;
-    const StageMeta& m = sm.st[0];
+    uint32_t* P = stage_buf(sm, s);
+    const uint32_t* Pprev = stage_buf(sm, s ^ 1);
+    if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u << s;
+    const StageMeta& m = sm.st[s];
     if (m.g >= src.total) break;
     const int item = m.item;
     const OpArgs& A = src.args(item);
     const long long c = m.c;
     const int nw = m.nw;
-    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, Cprev, true, raw_word_of); };
+    // a raw chunk's payload is its requantized words, kept swizzled in its buffer
+    auto raw_prev = [Pprev](const OpArgs&, long long, int w) -> uint32_t { return Pprev[swz(w)]; };
+    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, reinterpret_cast<const uint8_t*>(Pprev), raw_prev); };
     uint32_t v[32];
     bool raw;
     if (nw == CW) decode_core<true>(sm, A.sy, m, P, C, v, raw, NoHook{});
@@ -495,30 +502,62 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
       const Quant qs = make_quant(m.eb_e);
       const Quant q1 = A.q1, q2 = A.q2;
+      // Shift form, when every word of the warp allows it: a lossy stored bin
+      // a (|a| < 2^23) is the float a * 2^(e_s - 126), so its request bin is
+      // a / 2^k1 rounded half away from zero (k1 = e_1 - e_s >= 0), and the
+      // residual is a / 2^k2 (rounded) minus that request bin moved to the
+      // destination's bins, (a / 2^k1 rounded) << (e_1 - e_2), exact while the
+      // latter stays a lossy destination bin (magnitudes below `amax`).
+      const int k1 = q1.eb_e - qs.eb_e;
+      const int k2 = (OP == OP_RESI) ? q2.eb_e - qs.eb_e : 0;
+      const int dd = (OP == OP_RESI) ? q1.eb_e - q2.eb_e : 0;
+      const bool shift_ok = !raw && k1 >= 0 && k2 >= 0 && dd >= 0;
+      const uint32_t amax =
+          (OP == OP_RESI && k2 == 0 && k1 >= 1 && k1 <= 23) ? 0x800000u - (1u << (k1 - 1)) : 0x800000u;
+      uint32_t big = 0;
 #pragma unroll
       for (int k = 0; k < 32; k++) {
-        const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
-        if (OP == OP_S2C) {
-          v[k] = cq_enc(x, q1);
-        } else {
-          const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
-          v[k] = cq_enc(x, q2) - src_req;
+        const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
+        big = max(big, (v[k] ^ neg) - neg);
+      }
+      if (__all_sync(0xffffffffu, shift_ok && big < amax)) {
+        const uint32_t h1 = shl_clamp(1u, (uint32_t)(k1 - 1)), h2 = shl_clamp(1u, (uint32_t)(k2 - 1));
+#pragma unroll
+        for (int k = 0; k < 32; k++) {
+          const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
+          const uint32_t a = (v[k] ^ neg) - neg;
+          const uint32_t m1 = shr_clamp(a + h1, (uint32_t)k1);
+          const uint32_t r = (OP == OP_S2C) ? m1 : shr_clamp(a + h2, (uint32_t)k2) - shl_clamp(m1, (uint32_t)dd);
+          v[k] = (r ^ neg) - neg;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) {
+          const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+          if (OP == OP_S2C) {
+            v[k] = cq_enc(x, q1);
+          } else {
+            const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
+            v[k] = cq_enc(x, q2) - src_req;
+          }
         }
       }
       row_store(P, tid, v);  // raw source: the bins / residuals
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
       if (nw == CW) {
-        encode_stage<true>(sm, A.sy, v, C, P, c, nw, item, sm.pend[s], flush_prev);
+        encode_stage<true>(sm, A.sy, v, C, reinterpret_cast<uint8_t*>(P), c, nw, item, sm.pend[s], flush_prev);
       } else {
-        encode_stage_partial(sm, A.sy, v, C, P, c, nw, item, sm.pend[s]);
         flush_prev();
+        encode_stage_partial(sm, A.sy, v, C, reinterpret_cast<uint8_t*>(P), c, nw, item, sm.pend[s]);
       }
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
-    __syncthreads();  // buffer 0 (payload, raw copy) and the flushed staging are free
-    take_next();
+    __syncthreads();  // buffer s^1 (flushed) and buffer 2 are free
+    take_next(s ^ 1);
   }
-  flush_pending(sm, src, s ^ 1, stage_buf(sm, 2 - s), true, raw_word_of);
+  const uint32_t* Pl = stage_buf(sm, s ^ 1);
+  flush_pending(sm, src, s ^ 1, reinterpret_cast<const uint8_t*>(Pl),
+                [Pl](const OpArgs&, long long, int w) -> uint32_t { return Pl[swz(w)]; });
 }
 
 // storage decode / init_recv / resi_recv (d_server_decode_kernel,

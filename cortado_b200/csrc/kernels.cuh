@@ -138,30 +138,70 @@ __device__ __forceinline__ void plane_offsets(int tid, uint32_t& e, uint32_t& o)
   o = 32 * warp + ((((lane >> 2) & 7u) ^ (warp + 4)) << 2) + (lane & 3);
 }
 
+// ---------------------------------------------------------------- rotated walks
+// Zero elimination moves each thread's bytes to a contiguous region that
+// starts wherever the previous thread's ended.  For dense data those regions
+// are about 128 bytes apart, so threads that walk their 32 words in the same
+// order store to the same shared-memory bank (a 32-way conflict).  The
+// compaction of a dense warp therefore walks each thread's words starting at
+// word `lane`: nibble j of the rotated mask (rot_nibbles) belongs to word
+// (lane + j) % 32, and nibble_prefix gives the byte count before the starting
+// word.
+
+// Bytes before word k of a segment: the set bits of the 4-bit-per-word mask
+// M (128 bits) below nibble k.
+__device__ __forceinline__ uint32_t nibble_prefix(const uint32_t (&M)[4], int k) {
+  const int nb = 4 * k;
+  uint32_t c = 0;
+#pragma unroll
+  for (int w = 0; w < 4; w++) {
+    const int lim = nb - 32 * w;
+    const uint32_t mask = lim >= 32 ? 0xffffffffu : (lim <= 0 ? 0u : (1u << lim) - 1u);
+    c += __popc(M[w] & mask);
+  }
+  return c;
+}
+
+// The 128-bit mask M rotated right by 4*r bits.
+__device__ __forceinline__ void rot_nibbles(const uint32_t (&M)[4], int r, uint32_t (&R)[4]) {
+  uint32_t a0 = M[0], a1 = M[1], a2 = M[2], a3 = M[3];
+  if (r & 8) {
+    const uint32_t t = a0;
+    a0 = a1; a1 = a2; a2 = a3; a3 = t;
+  }
+  if (r & 16) {
+    uint32_t t = a0; a0 = a2; a2 = t;
+    t = a1; a1 = a3; a3 = t;
+  }
+  const uint32_t bs = 4 * (r & 7);
+  R[0] = __funnelshift_r(a0, a1, bs);
+  R[1] = __funnelshift_r(a1, a2, bs);
+  R[2] = __funnelshift_r(a2, a3, bs);
+  R[3] = __funnelshift_r(a3, a0, bs);
+}
+
 // ============================================================== encode stage
 // Input: v[32] = the pre-DIFFMS words of group g = threadIdx.x (quantized bins
 // or residuals; words at or beyond nw are 0).  `plane` is a swizzled 16 KiB
 // buffer that may be overwritten once every thread has passed the first
-// barrier; it becomes the plane buffer and then the staging of the compacted
-// payload (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1, raw fallback).  The chunk's size
-// is published for the lookback; the payload is written out later by
-// flush_chunk, once the size of every earlier chunk is known.  raw_copy, when
-// not null, is a swizzled buffer holding the pre-DIFFMS words, copied (linear)
-// into the staging buffer when the chunk does not compress; otherwise a raw
-// chunk's words are read back from the input by the flush.  The chunk is
+// barrier; it becomes the plane buffer (d_DIFFMS_4 -> d_BIT_4 -> d_RZE_1, raw
+// fallback).  The compacted payload goes to `staging` (linear bytes), which
+// the caller may still be reading until after_publish() returns.  The chunk's
+// size is published for the lookback; the payload is written out later by
+// flush_chunk, once the size of every earlier chunk is known (a raw chunk's
+// words are read back from wherever the caller keeps them).  The chunk is
 // recorded in `pend`.  after_publish() runs on every thread once the size is
 // published (it may hold barriers: the pipelined loops flush the previous
 // chunk there, a whole iteration after that chunk's own publication).
 // FULL: a whole 16 KiB chunk (nw == 4096), with compile-time addressing.
 template <bool FULL, typename Hook>
 __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (&v)[32], uint32_t* plane,
-                                             const uint32_t* raw_copy, long long c, int nw_in, int item,
-                                             Pend& pend, Hook after_publish) {
+                                             uint8_t* st, long long c, int nw_in, int item, Pend& pend,
+                                             Hook after_publish) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = FULL ? CW : nw_in;
   const int osize = nw * 4;
   const int G = nw >> 5, rem = nw & 31;
-  uint8_t* st = reinterpret_cast<uint8_t*>(plane);
 
   // DIFFMS (d_DIFFMS.h:44-66): word minus its predecessor, then zig-zag.
   if (lane == 31) sm.xchg[warp] = v[31];
@@ -174,11 +214,13 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
     // RZE_1 emits only its 2-byte trailer (the original chunk size).
     if (tid == 0) {
       lookback_publish(sy, sm.epoch, c, 2u);
-      st[0] = (uint8_t)osize;
-      st[1] = (uint8_t)(osize >> 8);
       pend = Pend{c, item, nw, 2, 0, 1};
     }
     after_publish();
+    if (tid == 0) {
+      st[0] = (uint8_t)osize;
+      st[1] = (uint8_t)(osize >> 8);
+    }
     return;
   }
   uint32_t prev = __shfl_up_sync(0xffffffffu, v[31], 1);
@@ -287,12 +329,7 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
     pend = Pend{c, item, nw, (int)csize, (int)raw, 1};
   }
   after_publish();
-  if (raw) {
-    if (raw_copy) {
-      for (int w = tid; w < nw; w += NT) plane[w] = raw_copy[swz(w)];
-    }
-    return;
-  }
+  if (raw) return;
   if (warp == 0) {
     if (NZ == 0) {
       if (lane == 0) {
@@ -311,7 +348,11 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
     }
   }
   // Compaction of the zero-eliminated bytes and the kept level-1 bitmap bytes.
-  if (nz) {
+  // When many lanes of the warp hold data, the words are read back from the
+  // plane buffer in the lane-rotated order (conflict-free stores); otherwise
+  // they come from registers in order.
+  const bool dense = __popc(__ballot_sync(0xffffffffu, nz > 16)) >= 2;
+  if (nz && !dense) {
     uint32_t p = zoff;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
@@ -326,6 +367,32 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
 #pragma unroll
         for (int b = 0; b < 4; b++)
           if ((m >> b) & 1) st[p++] = (uint8_t)(q[k] >> (8 * b));
+      }
+    }
+  } else if (nz) {
+    uint32_t R[4];
+    rot_nibbles(M, lane, R);
+    uint32_t rel = nibble_prefix(M, lane);
+    const uint32_t rowbase = 32u * tid;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const uint32_t k = (lane + j) & 31;
+      if (k == 0) rel = 0;
+      const uint32_t m = (R[j >> 3] >> (4 * (j & 7))) & 15u;
+      if (m) {
+        const uint32_t w = plane[swz(rowbase + k)];
+        uint32_t p = zoff + rel;
+        if (m == 15u) {
+          st[p] = (uint8_t)w;
+          st[p + 1] = (uint8_t)(w >> 8);
+          st[p + 2] = (uint8_t)(w >> 16);
+          st[p + 3] = (uint8_t)(w >> 24);
+        } else {
+#pragma unroll
+          for (int b = 0; b < 4; b++)
+            if ((m >> b) & 1) st[p++] = (uint8_t)(w >> (8 * b));
+        }
+        rel += __popc(m);
       }
     }
   }
@@ -560,13 +627,12 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
 // The partial last chunk of a stream (at most one per stream) runs out of
 // line, so the full-chunk loop body stays small enough for the instruction
 // caches.  Arrays pass through local memory on this rare path.
-__device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint32_t* v, uint32_t* plane,
-                                                  const uint32_t* raw_copy, long long c, int nw, int item,
-                                                  Pend& pend) {
+__device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint32_t* v, uint32_t* plane, uint8_t* st,
+                                                  long long c, int nw, int item, Pend& pend) {
   uint32_t w[32];
 #pragma unroll
   for (int k = 0; k < 32; k++) w[k] = v[k];
-  encode_stage<false>(sm, sy, w, plane, raw_copy, c, nw, item, pend, NoHook{});
+  encode_stage<false>(sm, sy, w, plane, st, c, nw, item, pend, NoHook{});
 }
 
 template <typename Side>
