@@ -353,21 +353,22 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
   // they come from registers in order.
   const bool dense = __popc(__ballot_sync(0xffffffffu, nz > 16)) >= 2;
   if (nz && !dense) {
+    // only the non-zero words, in order: bit k of wm <-> word k has a byte
+    uint32_t wm = 0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) wm |= (((M[k >> 3] >> (4 * (k & 7))) & 15u) != 0u ? 1u : 0u) << k;
     uint32_t p = zoff;
-#pragma unroll
-    for (int k = 0; k < 32; k++) {
+    const uint32_t rowbase = 32u * tid;
+    while (wm) {
+      const uint32_t k = __ffs(wm) - 1;
+      wm &= wm - 1;
       const uint32_t m = (M[k >> 3] >> (4 * (k & 7))) & 15u;
-      if (m == 15u) {
-        st[p] = (uint8_t)q[k];
-        st[p + 1] = (uint8_t)(q[k] >> 8);
-        st[p + 2] = (uint8_t)(q[k] >> 16);
-        st[p + 3] = (uint8_t)(q[k] >> 24);
-        p += 4;
-      } else if (m) {
-#pragma unroll
-        for (int b = 0; b < 4; b++)
-          if ((m >> b) & 1) st[p++] = (uint8_t)(q[k] >> (8 * b));
-      }
+      const uint32_t w = plane[swz(rowbase + k)];
+      if (m & 1u) st[p] = (uint8_t)w;
+      if (m & 2u) st[p + (m & 1u)] = (uint8_t)(w >> 8);
+      if (m & 4u) st[p + __popc(m & 3u)] = (uint8_t)(w >> 16);
+      if (m & 8u) st[p + __popc(m & 7u)] = (uint8_t)(w >> 24);
+      p += __popc(m);
     }
   } else if (nz) {
     uint32_t R[4];
