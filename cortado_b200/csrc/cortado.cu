@@ -84,6 +84,7 @@ __device__ __forceinline__ unsigned int finish_launch(Ctl& sm, const Sync& sy, b
       *sy.epoch = (e == 65535u) ? 0u : e + 1u;
       sy.counter[0] = 0;
       sy.counter[1] = 0;
+      sy.counter[6] = 0;
       __threadfence();
     }
   }
@@ -664,10 +665,20 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
   if (tid == TMA_TID) bulk_wait_read();
 }
 
-// ---- the helper CTA of a launch (its last CTA, when there are at least two):
-// warp 0 runs the lookback resolver (encoders), warp 1 the offset scanner
-// (stream inputs).  A one-CTA launch scans its offsets itself first.
-__device__ __forceinline__ bool helper_cta() { return gridDim.x >= 2 && blockIdx.x == gridDim.x - 1; }
+// ---- the helper CTA of a launch (the first CTA to start, when there are at
+// least two): warp 0 runs the lookback resolver (encoders), warp 1 the offset
+// scanner (stream inputs).  Being the first to start, it is resident even
+// when other kernels share the GPU and not every CTA of the launch fits at
+// once, so the CTAs that wait for its offsets cannot wait for a CTA that
+// waits for them.  A one-CTA launch scans its offsets itself first.
+__device__ __forceinline__ bool helper_cta(Ctl& sm, const Sync& sy) {
+  if (gridDim.x < 2) return false;
+  if (threadIdx.x == 0) sm.is_last = atomicAdd(&sy.counter[6], 1u) == 0;
+  __syncthreads();
+  const bool h = sm.is_last;
+  __syncthreads();
+  return h;
+}
 
 template <bool RESOLVE, bool SCAN, class Src>
 __device__ __forceinline__ void run_helper(Ctl& sm, const Src& src, const Sync& sy) {
@@ -687,7 +698,7 @@ __global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant_
     if (chunks == 0) *a.out_size = HDR;
   }
   const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
-  if (helper_cta()) run_helper<true, false>(sm, src, a.sy);
+  if (helper_cta(sm, a.sy)) run_helper<true, false>(sm, src, a.sy);
   else store_loop(sm, src, a.sy);
   finish_launch(sm, a.sy);
 }
@@ -704,7 +715,7 @@ __global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_consta
     if (h.chunks == 0) *a.out_size = HDR;
   }
   const SingleSrc src{&a, nullptr, nullptr, h.chunks, h};
-  if (helper_cta()) run_helper<true, true>(sm, src, a.sy);
+  if (helper_cta(sm, a.sy)) run_helper<true, true>(sm, src, a.sy);
   else reencode_loop<OP>(sm, src, a.sy);
   finish_launch(sm, a.sy);
 }
@@ -722,7 +733,7 @@ __global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) 
     *a.out_size = hdr_ok ? h.n : 0;
   }
   const SingleSrc src{&a, &map_src, &map_out, h.chunks, h};
-  if (helper_cta()) run_helper<false, true>(sm, src, a.sy);
+  if (helper_cta(sm, a.sy)) run_helper<false, true>(sm, src, a.sy);
   else decode_loop<OP>(sm, src, a.sy);
   finish_launch(sm, a.sy);
 }
@@ -734,7 +745,7 @@ k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks
   Ctl& sm = ctl_block();
   const BatchSrc<OP> src{items, n_items, total_chunks};
   constexpr bool encoder = OP == OP_STORE || OP == OP_S2C || OP == OP_RESI;
-  if (helper_cta()) run_helper<encoder, OP != OP_STORE>(sm, src, sy);
+  if (helper_cta(sm, sy)) run_helper<encoder, OP != OP_STORE>(sm, src, sy);
   else if (OP == OP_STORE) store_loop(sm, src, sy);
   else if (encoder) reencode_loop<OP>(sm, src, sy);
   else decode_loop<OP>(sm, src, sy);
@@ -744,7 +755,8 @@ k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks
 // ---- store without allocation (cortado_store_encode_noalloc)
 // Fixed scratch for callers that cannot allocate device memory: one
 // lookback word per chunk for up to CORTADO_NOALLOC_MAX_BYTES of input, then
-// the chunk queue, the finished-CTA count, the status word and the epoch.  Every GPU that
+// the chunk queue, the finished-CTA count, the status word, the epoch and the
+// helper ticket (32-bit words 0, 1, 2, 3 and 6 of the last 4 entries).  Every GPU that
 // loads the library holds this array until the process exits.
 constexpr long long NOALLOC_CHUNKS = CORTADO_NOALLOC_MAX_BYTES / CS;
 __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_CHUNKS + 4];
@@ -761,7 +773,7 @@ __global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_c
     if (chunks == 0) *a.out_size = HDR;
   }
   const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
-  if (helper_cta()) run_helper<true, false>(sm, src, a.sy);
+  if (helper_cta(sm, a.sy)) run_helper<true, false>(sm, src, a.sy);
   else store_loop(sm, src, a.sy);
   const unsigned int st = finish_launch(sm, a.sy, true);
   if (st) *a.out_size = -(long long)st;
@@ -825,7 +837,7 @@ struct cortado_ctx {
   int grid_store = 0, grid_reenc = 0, grid_dec = 0, grid_rapply = 0;
   unsigned long long* flags = nullptr;
   long long flags_cap = 0;
-  unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax, [5] epoch
+  unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax, [5] epoch, [6] helper ticket
   int grid_batch[6] = {0, 0, 0, 0, 0, 0};
   int ctas_override[6] = {0, 0, 0, 0, 0, 0};  // per op: resident CTAs per SM (0 = occupancy limit)
   // Item tables of the batched launch: a ring of ITEM_SLOTS slots, each with

@@ -56,7 +56,7 @@ struct Sync {
   unsigned long long* flags;  // lookback words, one per chunk (encoders)
   unsigned long long* offs;   // input payload offsets, one per chunk (decoders, re-encoders), or null
   long long flags_cap;        // words in flags and in offs (cleared when the epoch wraps)
-  unsigned int* counter;      // [0] chunk queue, [1] CTAs finished
+  unsigned int* counter;      // [0] chunk queue, [1] CTAs finished, [6] helper ticket
   unsigned int* status;       // first error latched
   unsigned int* epoch;        // 0..65535, tags this launch's lookback words
   unsigned long long timeout_ns;
@@ -228,6 +228,18 @@ __device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
 __device__ __forceinline__ uint32_t nz_nibble(uint32_t x) {
   const uint32_t h = (((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x) & 0x80808080u;
   return ((h >> 7) * 0x01020408u) >> 24;
+}
+// 8-bit mask of the non-zero nibbles of x (bit i <-> nibble i).
+__device__ __forceinline__ uint32_t nz_nibbles8(uint32_t x) {
+  uint32_t h = ((((x & 0x77777777u) + 0x77777777u) | x) & 0x88888888u) >> 3;
+  h = (h | (h >> 3)) & 0x03030303u;
+  h = (h | (h >> 6)) & 0x000f000fu;
+  return (h | (h >> 12)) & 0xffu;
+}
+// Nibble k (0..31) of a 128-bit mask held in four words.
+__device__ __forceinline__ uint32_t nibble_at(const uint32_t (&M)[4], uint32_t k) {
+  const uint32_t w = (k < 16) ? ((k < 8) ? M[0] : M[1]) : ((k < 24) ? M[2] : M[3]);
+  return (w >> (4 * (k & 7))) & 15u;
 }
 // Byte-permute selector that scatters the first popc(m) bytes of a word to
 // the positions of the set bits of m and zero-fills the others.

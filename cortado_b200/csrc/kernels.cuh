@@ -354,15 +354,13 @@ __device__ __forceinline__ void encode_stage(Ctl& sm, const Sync& sy, uint32_t (
   const bool dense = __popc(__ballot_sync(0xffffffffu, nz > 16)) >= 2;
   if (nz && !dense) {
     // only the non-zero words, in order: bit k of wm <-> word k has a byte
-    uint32_t wm = 0;
-#pragma unroll
-    for (int k = 0; k < 32; k++) wm |= (((M[k >> 3] >> (4 * (k & 7))) & 15u) != 0u ? 1u : 0u) << k;
+    uint32_t wm = nz_nibbles8(M[0]) | (nz_nibbles8(M[1]) << 8) | (nz_nibbles8(M[2]) << 16) | (nz_nibbles8(M[3]) << 24);
     uint32_t p = zoff;
     const uint32_t rowbase = 32u * tid;
     while (wm) {
       const uint32_t k = __ffs(wm) - 1;
       wm &= wm - 1;
-      const uint32_t m = (M[k >> 3] >> (4 * (k & 7))) & 15u;
+      const uint32_t m = nibble_at(M, k);
       const uint32_t w = plane[swz(rowbase + k)];
       if (m & 1u) st[p] = (uint8_t)w;
       if (m & 2u) st[p + (m & 1u)] = (uint8_t)(w >> 8);
