@@ -6,11 +6,12 @@
 //   init_recv      include/d_client_encode.h:173-259
 //   resi_send      include/d_residual_encode.h:51-201
 //   resi_recv      include/d_residual_encode.h:238-347
-// Differences in mechanism (not in output bytes): chunk offsets from a bounded,
-// epoch-tagged decoupled lookback (encoders) or a per-CTA running sum of the
-// size table (decoders); one 128-thread CTA per chunk with the data held in
-// registers; TMA for float chunks and compressed payloads, prefetched one
-// chunk ahead; errors latched in a status word instead of printf + __trap.
+// Differences in mechanism (not in output bytes): output offsets from a
+// bounded, epoch-tagged decoupled lookback, resolved one chunk later
+// (encoders), and input offsets from a prefix sum of the size table computed
+// once per launch (decoders, re-encoders); one 128-thread CTA per chunk with
+// the data held in registers; TMA for float chunks and compressed payloads;
+// errors latched in a status word instead of printf + __trap.
 #pragma once
 #include "device.cuh"
 
@@ -34,10 +35,8 @@ struct OpArgs {
 // ---------------------------------------------------------------- shared memory
 // A CTA owns a 1 KiB control block followed by 2 or 3 chunk buffers of
 // BUF_WORDS words (16 KiB + slack, a multiple of 1024 bytes so that every
-// buffer keeps the 1024-byte alignment TMA's 128B swizzle needs).  Buffers 0
-// and 1 are the two pipeline stages (the chunk being processed and the one
-// being loaded); buffer 2 is the re-encoders' plane buffer or resi_recv's
-// client chunk.
+// buffer keeps the 1024-byte alignment TMA's 128B swizzle needs).  How the
+// loops use them is described at each loop (cortado.cu).
 constexpr int BUF_WORDS = 4352;
 constexpr int CTL_BYTES = 1024;
 
