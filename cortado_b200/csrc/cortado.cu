@@ -300,14 +300,22 @@ __device__ __forceinline__ void prefetch_stream(Ctl& sm, int t, long long g, con
   const uint8_t* data = A.in + HDR + 2 * chunks;
   const long long data_bytes = A.in_bytes - HDR - 2 * chunks;
   unsigned long long off = 0;
-  if (lane == 0) off = wait_offset(A.sy, sm.epoch, c);
+  int cs = 0;
+  if (lane == 0) {
+    cs = table[c];  // in flight together with the offset read
+    off = wait_offset(A.sy, sm.epoch, c);
+  }
   off = __shfl_sync(0xffffffffu, off, 0);
-  const int cs = table[c];
+  cs = __shfl_sync(0xffffffffu, cs, 0);
   const int bad = (cs > osize) || (cs < 2 && cs != osize) || ((long long)off + cs > data_bytes);
   const uintptr_t Aa = reinterpret_cast<uintptr_t>(data + off);
   const uintptr_t a0 = Aa & ~uintptr_t(15);
   uintptr_t a1 = (Aa + (bad ? 0 : cs)) & ~uintptr_t(15);
   if (a1 < a0) a1 = a0;
+  // The copy may run into the next payload's bytes: it takes the ragged tail
+  // too unless that would read past the stream's valid bytes.
+  const uintptr_t a1_up = (Aa + (bad ? 0 : cs) + 15) & ~uintptr_t(15);
+  if (!bad && a1_up <= reinterpret_cast<uintptr_t>(A.in + A.in_bytes)) a1 = a1_up;
   const int d = (int)(Aa - a0);
   const int tma_len = (int)(a1 - a0);
   uint8_t* dst = reinterpret_cast<uint8_t*>(stage_buf(sm, t));
