@@ -17,13 +17,13 @@ using namespace cortado;
 
 // ================================================================== kernels
 // Resident CTAs per SM each kernel is compiled for (register budget
-// 65536 / (128 * n)).  init_send, resi_send and resi_recv hold a third 17 KiB
-// buffer, so shared memory limits them to 4.
+// 65536 / (128 * n)).  resi_recv holds a third 17 KiB buffer (the client's
+// chunk), so shared memory limits it to 4.
 #ifndef MINB_STORE
 #define MINB_STORE 6
 #endif
 #ifndef MINB_REENC
-#define MINB_REENC 4
+#define MINB_REENC 6
 #endif
 #ifndef MINB_DEC
 #define MINB_DEC 6
@@ -459,9 +459,12 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
 
 // init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
 // decode the stored chunk, requantize or form the residual, encode.  The
-// payload of the chunk in stage s arrives in buffer s, which then holds the
-// requantized words (the raw fallback) and finally the compacted payload until
-// the next iteration flushes it; buffer 2 is the plane buffer of both halves.
+// payload arrives in buffer 0 and is expanded in place; after the
+// requantization the same buffer is the encoder's plane buffer.  The compacted
+// payload goes to buffer 1 once the previous chunk has been flushed from there
+// (as in store_loop).  A chunk that does not compress stores its requantized
+// words, which are rebuilt from the plane buffer (planes_to_words) into
+// buffer 1 -- rare enough not to keep a third buffer for them.
 template <int OP, class Src>
 __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -474,35 +477,38 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
   __syncthreads();  // sm.epoch
   if (gridDim.x == 1 && warp == 1) src.scan(sm.epoch);
   __syncthreads();
-  auto take_next = [&](int t) {
+  uint32_t* X = stage_buf(sm, 0);
+  uint32_t* Yw = stage_buf(sm, 1);
+  uint8_t* Y = reinterpret_cast<uint8_t*>(Yw);
+  // a raw chunk's payload is its requantized words, kept swizzled in buffer 1
+  auto raw_word = [Yw](const OpArgs&, long long, int w) -> uint32_t { return Yw[swz(w)]; };
+  auto take_next = [&]() {
     if (warp == 3) {
       long long g = 0;
       if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
-      prefetch_stream(sm, t, __shfl_sync(0xffffffffu, g, 0), src, ws);
+      prefetch_stream(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
     }
   };
-  take_next(0);
-  uint32_t* C = stage_buf(sm, 2);
+  take_next();
   uint32_t phase = 0;
-  int s = 0;
+  int s = 0;  // pending-chunk slot of this iteration's chunk
   for (;; s ^= 1) {
-    uint32_t* P = stage_buf(sm, s);
-    const uint32_t* Pprev = stage_buf(sm, s ^ 1);
-    if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
-    phase ^= 1u << s;
-    const StageMeta& m = sm.st[s];
+    if (!mbar_wait(&sm.bar[0], phase & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
+    phase ^= 1u;
+    const StageMeta& m = sm.st[0];
     if (m.g >= src.total) break;
     const int item = m.item;
     const OpArgs& A = src.args(item);
     const long long c = m.c;
     const int nw = m.nw;
-    // a raw chunk's payload is its requantized words, kept swizzled in its buffer
-    auto raw_prev = [Pprev](const OpArgs&, long long, int w) -> uint32_t { return Pprev[swz(w)]; };
-    auto flush_prev = [&]() { flush_pending(sm, src, s ^ 1, reinterpret_cast<const uint8_t*>(Pprev), raw_prev); };
+    auto flush_prev = [&]() {
+      flush_pending(sm, src, s ^ 1, Y, raw_word);
+      __syncthreads();  // buffer 1 has been read
+    };
     uint32_t v[32];
     bool raw;
-    if (nw == CW) decode_core<true>(sm, A.sy, m, P, C, v, raw, NoHook{});
-    else decode_core_partial(sm, A.sy, m, P, C, v, raw, NoHook{});
+    if (nw == CW) decode_core<true>(sm, A.sy, m, X, X, v, raw, NoHook{});
+    else decode_core_partial(sm, A.sy, m, X, X, v, raw, NoHook{});
     if (m.bad >= 2) {  // unusable stream header (batched): nothing to write
       if (tid == 0) sm.pend[s].valid = 0;
       flush_prev();
@@ -551,22 +557,26 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
           }
         }
       }
-      row_store(P, tid, v);  // raw source: the bins / residuals
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
       if (nw == CW) {
-        encode_stage<true>(sm, A.sy, v, C, reinterpret_cast<uint8_t*>(P), c, nw, item, sm.pend[s], flush_prev);
+        encode_stage<true>(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s], flush_prev);
       } else {
         flush_prev();
-        encode_stage_partial(sm, A.sy, v, C, reinterpret_cast<uint8_t*>(P), c, nw, item, sm.pend[s]);
+        encode_stage_partial(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s]);
+        __syncthreads();  // sm.pend[s]
+      }
+      if (sm.pend[s].raw) {
+        // the requantized words, rebuilt from the plane buffer, are the payload
+        if (nw == CW) planes_to_words<true>(sm, X, nw, v);
+        else planes_to_words_partial(sm, X, nw, v);
+        row_store(Yw, tid, v);
       }
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
-    __syncthreads();  // buffer s^1 (flushed) and buffer 2 are free
-    take_next(s ^ 1);
+    __syncthreads();  // buffer 0 has been read; buffer 1 holds this chunk's payload
+    take_next();
   }
-  const uint32_t* Pl = stage_buf(sm, s ^ 1);
-  flush_pending(sm, src, s ^ 1, reinterpret_cast<const uint8_t*>(Pl),
-                [Pl](const OpArgs&, long long, int w) -> uint32_t { return Pl[swz(w)]; });
+  flush_pending(sm, src, s ^ 1, Y, raw_word);
 }
 
 // storage decode / init_recv / resi_recv (d_server_decode_kernel,
@@ -964,8 +974,8 @@ int occupancy_grid(K kernel, size_t smem, int sms) {
   return per * sms;
 }
 
-constexpr size_t SMEM_STD = smem_bytes(2);  // store, storage decode, init_recv
-constexpr size_t SMEM_SRC = smem_bytes(3);  // init_send, resi_send, resi_recv
+constexpr size_t SMEM_STD = smem_bytes(2);  // store, init_send, resi_send, storage decode, init_recv
+constexpr size_t SMEM_SRC = smem_bytes(3);  // resi_recv (+ the client's chunk)
 
 cortado_status launch_status(cudaError_t e) { return from_cuda(e == cudaSuccess ? cudaGetLastError() : e); }
 
@@ -1016,14 +1026,14 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   if (e != cudaSuccess) { delete ctx; return from_cuda(e); }
   cudaMemset(ctx->words, 0, 64);
   ctx->grid_store = occupancy_grid(k_store, SMEM_STD, ctx->sms);
-  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_SRC, ctx->sms);
-  occupancy_grid(k_reencode<OP_RESI>, SMEM_SRC, ctx->sms);
+  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
   ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
   occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_SRC, ctx->sms);
   ctx->grid_batch[OP_STORE] = occupancy_grid(k_batch<OP_STORE>, SMEM_STD, ctx->sms);
-  ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_SRC, ctx->sms);
-  ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_SRC, ctx->sms);
+  ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_STD, ctx->sms);
+  ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_SRC, ctx->sms);
@@ -1123,8 +1133,8 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.q2 = make_quant(e2);
   a.sy = next_sync(ctx, st);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
-  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_SRC, st>>>(a);
-  else k_reencode<OP_RESI><<<grid, NT, SMEM_SRC, st>>>(a);
+  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
+  else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
   return launch_status(cudaSuccess);
 }
 
@@ -1324,7 +1334,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   cudaError_t e = cudaMemcpyAsync(d_tab, h_tab, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return from_cuda(e);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_batch[op]), total);
-  const size_t smem = (op == CORTADO_OP_RESI_RECV || op == CORTADO_OP_INIT_SEND || op == CORTADO_OP_RESI_SEND) ? SMEM_SRC : SMEM_STD;
+  const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_SRC : SMEM_STD;
   switch (op) {
     case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
     case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;

@@ -423,6 +423,55 @@ __device__ __forceinline__ void flush_chunk(const Ctl& sm, const Pend& p, const 
   }
 }
 
+// Inverse of DIFFMS + BIT_4 for a chunk whose BIT_4 output sits in the
+// swizzled plane buffer: gathers the plane words of group g = threadIdx.x,
+// transposes them back, undoes the zig-zag and the differences (in-thread
+// prefix sum plus a block scan of the group totals), and returns the group's
+// words in v[32] (words at or beyond nw are 0).  Ends with a barrier (the
+// scan's), after which the plane buffer may be reused.
+template <bool FULL>
+__device__ __forceinline__ void planes_to_words(Ctl& sm, const uint32_t* plane, int nw_in, uint32_t (&v)[32]) {
+  const int tid = threadIdx.x;
+  const int nw = FULL ? CW : nw_in;
+  const int G = nw >> 5, rem = nw & 31;
+  // ---- undo BIT_4 (d_iBIT_4): gather plane words of group g, transpose.
+  if (FULL) {
+    uint32_t pe, po;
+    plane_offsets(tid, pe, po);
+    uint32_t any = 0;
+#pragma unroll
+    for (int s = 0; s < 32; s++) {
+      v[s] = plane[128 * s + ((s & 1) ? po : pe)];
+      any |= v[s];
+    }
+    if (any) transpose32(v);
+  } else if (tid < G) {
+#pragma unroll
+    for (int s = 0; s < 32; s++) v[s] = plane[swz(s * G + tid)];
+    transpose32(v);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = (tid == G && k < rem) ? plane[swz(32 * G + k)] : 0u;
+  }
+  // ---- undo DIFFMS (d_iDIFFMS, d_DIFFMS.h:69-102): un-zig-zag, prefix sum.
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    const uint32_t z = v[k];
+    acc += (z >> 1) ^ (0u - (z & 1u));
+    v[k] = acc;
+  }
+  uint32_t dummy;
+  const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);  // (its barrier: every plane read is done)
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] += carry;
+  if (!FULL && 32 * tid + 32 > nw) {
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      if (32 * tid + k >= nw) v[k] = 0;
+  }
+}
+
 // ============================================================== decode stage
 // Undoes RZE_1, BIT_4 and DIFFMS for the chunk whose payload the stage's
 // loads brought into P (at byte offset m.d, m.csize bytes; see StageMeta) and
@@ -439,7 +488,6 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = FULL ? CW : m.nw;
   const int osize = nw * 4;
-  const int G = nw >> 5, rem = nw & 31;
   const bool inplace = plane == P;
   const uint8_t* st = reinterpret_cast<const uint8_t*>(P);
   const int csize = m.csize;
@@ -584,42 +632,7 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
   if (inplace) __syncthreads();  // every payload byte has been read
   row_store(plane, tid, q);
   __syncthreads();
-  // ---- undo BIT_4 (d_iBIT_4): gather plane words of group g, transpose.
-  if (FULL) {
-    uint32_t pe, po;
-    plane_offsets(tid, pe, po);
-    uint32_t any = 0;
-#pragma unroll
-    for (int s = 0; s < 32; s++) {
-      v[s] = plane[128 * s + ((s & 1) ? po : pe)];
-      any |= v[s];
-    }
-    if (any) transpose32(v);
-  } else if (tid < G) {
-#pragma unroll
-    for (int s = 0; s < 32; s++) v[s] = plane[swz(s * G + tid)];
-    transpose32(v);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = (tid == G && k < rem) ? plane[swz(32 * G + k)] : 0u;
-  }
-  // ---- undo DIFFMS (d_iDIFFMS, d_DIFFMS.h:69-102): un-zig-zag, prefix sum.
-  uint32_t acc = 0;
-#pragma unroll
-  for (int k = 0; k < 32; k++) {
-    const uint32_t z = v[k];
-    acc += (z >> 1) ^ (0u - (z & 1u));
-    v[k] = acc;
-  }
-  uint32_t dummy;
-  const uint32_t carry = block_scan_excl(acc, sm.scan_c, dummy);  // (its barrier: every plane read is done)
-#pragma unroll
-  for (int k = 0; k < 32; k++) v[k] += carry;
-  if (!FULL && 32 * tid + 32 > nw) {
-#pragma unroll
-    for (int k = 0; k < 32; k++)
-      if (32 * tid + k >= nw) v[k] = 0;
-  }
+  planes_to_words<FULL>(sm, plane, nw, v);
 }
 
 // The partial last chunk of a stream (at most one per stream) runs out of
@@ -631,6 +644,13 @@ __device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint3
 #pragma unroll
   for (int k = 0; k < 32; k++) w[k] = v[k];
   encode_stage<false>(sm, sy, w, plane, st, c, nw, item, pend, NoHook{});
+}
+
+__device__ __noinline__ void planes_to_words_partial(Ctl& sm, const uint32_t* plane, int nw, uint32_t* v) {
+  uint32_t w[32];
+  planes_to_words<false>(sm, plane, nw, w);
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = w[k];
 }
 
 template <typename Side>
