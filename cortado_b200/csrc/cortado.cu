@@ -817,33 +817,58 @@ __global__ void k_verify(const float* __restrict__ orig, const float* __restrict
   }
 }
 
-// ---- NOA range: min/max over the floats, NaNs ignored
-__global__ void k_minmax(const float* x, long long nw, unsigned int* out /* [2]: ordered-int min, max */) {
+// ---- NOA range: min/max over the floats, NaNs ignored (fminf/fmaxf skip
+// NaN operands).  Each thread keeps four 16-byte loads in flight per pass.
+__device__ __forceinline__ unsigned int ordered(float f) {
+  const unsigned int u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void __launch_bounds__(256) k_minmax(const float* x, long long nw, unsigned int* out /* [2]: ordered-int min, max */) {
   float mn = INFINITY, mx = -INFINITY;
   const long long nv = nw / 4;
   const float4* x4 = reinterpret_cast<const float4*>(x);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += stride) {
+  const long long nthr = (long long)gridDim.x * blockDim.x;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long i = t;
+  for (; i + 3 * nthr < nv; i += 4 * nthr) {
+    float4 v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) v[j] = __ldcs(x4 + i + j * nthr);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      mn = fminf(fminf(mn, v[j].x), fminf(v[j].y, fminf(v[j].z, v[j].w)));
+      mx = fmaxf(fmaxf(mx, v[j].x), fmaxf(v[j].y, fmaxf(v[j].z, v[j].w)));
+    }
+  }
+  for (; i < nv; i += nthr) {
     const float4 v = x4[i];
     mn = fminf(fminf(mn, v.x), fminf(v.y, fminf(v.z, v.w)));
     mx = fmaxf(fmaxf(mx, v.x), fmaxf(v.y, fmaxf(v.z, v.w)));
   }
-  for (long long i = 4 * nv + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += stride) {
-    mn = fminf(mn, x[i]);
-    mx = fmaxf(mx, x[i]);
+  for (long long k = 4 * nv + t; k < nw; k += nthr) {
+    mn = fminf(mn, x[k]);
+    mx = fmaxf(mx, x[k]);
   }
   for (int o = 16; o > 0; o >>= 1) {
     mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
     mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   }
-  auto ord = [](float f) -> unsigned int {
-    const unsigned int u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-  };
   if ((threadIdx.x & 31) == 0) {
-    atomicMin(&out[0], ord(mn));
-    atomicMax(&out[1], ord(mx));
+    atomicMin(&out[0], ordered(mn));
+    atomicMax(&out[1], ordered(mx));
   }
+}
+
+// Hands the range to the host through mapped pinned memory (a plain store,
+// no copy engine, so it is not queued behind bulk copies on other streams)
+// and resets the device words for the next call.
+__global__ void k_range_publish(unsigned int* words, volatile unsigned int* host) {
+  host[0] = words[0];
+  host[1] = words[1];
+  words[0] = 0xffffffffu;
+  words[1] = 0u;
+  __threadfence_system();
 }
 
 }  // namespace
@@ -868,6 +893,7 @@ struct cortado_ctx {
   int items_cap = 0;
   int items_slot = 0;
   cudaEvent_t items_done[ITEM_SLOTS] = {};
+  unsigned int* h_range = nullptr;  // mapped pinned host words: the last NOA range
   unsigned long long timeout_ns = 2000000000ull;
 };
 
@@ -1025,6 +1051,9 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   e = cudaMalloc(&ctx->words, 64);
   if (e != cudaSuccess) { delete ctx; return from_cuda(e); }
   cudaMemset(ctx->words, 0, 64);
+  cudaMemset(ctx->words + 3, 0xff, 4);  // NOA range words: min = all ones, max = 0
+  e = cudaHostAlloc((void**)&ctx->h_range, 8, cudaHostAllocMapped);
+  if (e != cudaSuccess) { cudaFree(ctx->words); delete ctx; return from_cuda(e); }
   ctx->grid_store = occupancy_grid(k_store, SMEM_STD, ctx->sms);
   ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_STD, ctx->sms);
   occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
@@ -1053,6 +1082,7 @@ void cortado_destroy(cortado_ctx* ctx) {
   cudaFree(ctx->words);
   cudaFree(ctx->d_items);
   cudaFreeHost(ctx->h_items);
+  cudaFreeHost(ctx->h_range);
   for (cudaEvent_t ev : ctx->items_done)
     if (ev) cudaEventDestroy(ev);
   delete ctx;
@@ -1219,17 +1249,16 @@ cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_b
                                  cortado_stream_t stream) {
   if (!ctx || !d_in || !h_min || !h_max || n_bytes <= 0 || (n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  unsigned int init[2] = {0xffffffffu, 0u};
-  cudaError_t e = cudaMemcpyAsync(ctx->words + 3, init, 8, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return from_cuda(e);
   const long long nw = n_bytes / 4;
-  long long blocks = (nw + 255) / 256;
-  if (blocks > 4L * ctx->sms) blocks = 4L * ctx->sms;
+  long long blocks = (nw / 4 + 1023) / 1024;
+  if (blocks > 8L * ctx->sms) blocks = 8L * ctx->sms;
+  if (blocks < 1) blocks = 1;
   k_minmax<<<(int)blocks, 256, 0, st>>>((const float*)d_in, nw, ctx->words + 3);
-  unsigned int r[2];
-  e = cudaMemcpyAsync(r, ctx->words + 3, 8, cudaMemcpyDeviceToHost, st);
+  k_range_publish<<<1, 1, 0, st>>>(ctx->words + 3, ctx->h_range);
+  cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return from_cuda(e);
+  const unsigned int r[2] = {((volatile unsigned int*)ctx->h_range)[0], ((volatile unsigned int*)ctx->h_range)[1]};
   auto unord = [](unsigned int o) -> float {
     const unsigned int u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
     float f;
