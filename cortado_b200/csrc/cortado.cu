@@ -17,8 +17,8 @@ using namespace cortado;
 
 // ================================================================== kernels
 // Resident CTAs per SM each kernel is compiled for (register budget
-// 65536 / (128 * n)).  resi_recv holds a third 17 KiB buffer (the client's
-// chunk), so shared memory limits it to 4.
+// 65536 / (128 * n)); every kernel holds two 17 KiB buffers, so shared memory
+// allows 6.
 #ifndef MINB_STORE
 #define MINB_STORE 6
 #endif
@@ -29,7 +29,7 @@ using namespace cortado;
 #define MINB_DEC 6
 #endif
 #ifndef MINB_RAPPLY
-#define MINB_RAPPLY 4
+#define MINB_RAPPLY 6
 #endif
 
 namespace {
@@ -581,8 +581,8 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
 
 // storage decode / init_recv / resi_recv (d_server_decode_kernel,
 // d_client_decode_kernel, d_residual_apply_kernel).  The payload is expanded
-// in place in its stage buffer, which then stages the output floats for one
-// TMA store; resi_recv's client chunk arrives in buffer 2.
+// in place in its stage buffer, which then takes resi_recv's client chunk and
+// stages the output floats for one TMA store.
 template <int OP, class Src>
 __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -600,7 +600,6 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
     if (lane == 0) pending = atomicAdd(&sy.counter[0], 1u);
   }
   __syncthreads();
-  uint32_t* S = stage_buf(sm, 2);
   uint32_t phase = 0;  // bits 0, 1: stages; bit 2: client chunk
   for (int s = 0;; s ^= 1) {
     const StageMeta& m = sm.st[s];
@@ -611,19 +610,6 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
     const int nw = m.nw;
     const bool full = nw == CW;
     uint32_t* P = stage_buf(sm, s);
-    bool src_tma = false;
-    if (OP == OP_RAPPLY && m.bad < 2) {
-      src_tma = full && A.has_map_in;
-      if (src_tma) {
-        if (tid == TMA_TID) {
-          fence_proxy_async();
-          mbar_expect_tx(&sm.bar_src, CS);
-          tma_load_rows(S, src.min(item), (int)(c * 128), &sm.bar_src);
-        }
-      } else {
-        load_plain_rows(S, A.src, c, nw);  // visible after the decoder's barriers
-      }
-    }
     if (Src::batched && c == 0 && tid == 0 && m.bad < 2) *A.out_size = m.n;
     if (!mbar_wait(&sm.bar[s], (phase >> s) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
     phase ^= 1u << s;
@@ -649,13 +635,24 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
     const Quant q = make_quant(m.eb_e);
     if (OP == OP_RAPPLY) {
       // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
-      // destination bound, add the residual, dequantize.
+      // destination bound, add the residual, dequantize.  The client's chunk
+      // comes into the stage buffer once the decoder has read it back.
+      __syncthreads();
+      const bool src_tma = full && A.has_map_in;
       if (src_tma) {
+        if (tid == TMA_TID) {
+          fence_proxy_async();
+          mbar_expect_tx(&sm.bar_src, CS);
+          tma_load_rows(P, src.min(item), (int)(c * 128), &sm.bar_src);
+        }
         if (!mbar_wait(&sm.bar_src, (phase >> 2) & 1, sy.timeout_ns)) latch(sy.status, DST_TIMEOUT);
         phase ^= 4u;
+      } else {
+        load_plain_rows(P, A.src, c, nw);
+        __syncthreads();
       }
       uint32_t s2[32];
-      row_load(S, tid, s2);
+      row_load(P, tid, s2);
 #pragma unroll
       for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s2[k], q) + v[k], q);
     } else if (!raw) {
@@ -1000,8 +997,7 @@ int occupancy_grid(K kernel, size_t smem, int sms) {
   return per * sms;
 }
 
-constexpr size_t SMEM_STD = smem_bytes(2);  // store, init_send, resi_send, storage decode, init_recv
-constexpr size_t SMEM_SRC = smem_bytes(3);  // resi_recv (+ the client's chunk)
+constexpr size_t SMEM_STD = smem_bytes(2);  // every encode / decode kernel
 
 cortado_status launch_status(cudaError_t e) { return from_cuda(e == cudaSuccess ? cudaGetLastError() : e); }
 
@@ -1059,13 +1055,13 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
   ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
   occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
-  ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_SRC, ctx->sms);
+  ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_STORE] = occupancy_grid(k_batch<OP_STORE>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
-  ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_SRC, ctx->sms);
+  ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_STD, ctx->sms);
   for (cudaEvent_t& ev : ctx->items_done) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   cortado_status s = ensure_flags(ctx, 1024, 0);
   cudaDeviceSynchronize();
@@ -1208,7 +1204,7 @@ static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int
   if (op == OP_RAPPLY) a.has_map_in = make_rows_map(&msrc, d_src, n_bytes);
   if (op == OP_SDEC) k_decode<OP_SDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
   else if (op == OP_CDEC) k_decode<OP_CDEC><<<grid_for(tuned_grid(ctx, op, ctx->grid_dec), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
-  else k_decode<OP_RAPPLY><<<grid_for(tuned_grid(ctx, op, ctx->grid_rapply), chunk_bound), NT, SMEM_SRC, st>>>(a, msrc, mout);
+  else k_decode<OP_RAPPLY><<<grid_for(tuned_grid(ctx, op, ctx->grid_rapply), chunk_bound), NT, SMEM_STD, st>>>(a, msrc, mout);
   return launch_status(cudaSuccess);
 }
 
@@ -1363,7 +1359,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   cudaError_t e = cudaMemcpyAsync(d_tab, h_tab, sizeof(BatchItem) * n_items, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return from_cuda(e);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_batch[op]), total);
-  const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_SRC : SMEM_STD;
+  const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_STD : SMEM_STD;
   switch (op) {
     case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
     case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
