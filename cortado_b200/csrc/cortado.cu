@@ -438,8 +438,20 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
     uint32_t v[32];
     row_load(A, tid, v);
     const Quant q1 = A_.q1;
+    {
+      // the float form when every word of the warp is below the lossless threshold
+      const FastQ fq = make_fastq(q1.eb_e);
+      uint32_t amax = 0;
 #pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], q1);
+      for (int k = 0; k < 32; k++) amax = max(amax, v[k] & 0x7fffffffu);
+      if (__all_sync(0xffffffffu, amax < fq.thr_bits)) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = sq_fast(v[k], fq);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], q1);
+      }
+    }
     auto flush_prev = [&]() {
       flush_pending(sm, src, s ^ 1, B, raw_word);
       __syncthreads();  // buffer 1 has been read
@@ -653,8 +665,31 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
       }
       uint32_t s2[32];
       row_load(P, tid, s2);
+      // float forms when every word of the warp is lossy (client float, then sum)
+      const FastQ fq = make_fastq(m.eb_e);
+      uint32_t amax = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = iq_dec(cq_enc(s2[k], q) + v[k], q);
+      for (int k = 0; k < 32; k++) amax = max(amax, s2[k] & 0x7fffffffu);
+      if (__all_sync(0xffffffffu, amax < fq.thr_bits)) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) s2[k] = cq_fast(s2[k], fq) + v[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) s2[k] = cq_enc(s2[k], q) + v[k];
+      }
+      uint32_t bmax = 0;
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        const uint32_t neg = (uint32_t)((int32_t)s2[k] >> 31);
+        bmax = max(bmax, (s2[k] ^ neg) - neg);
+      }
+      if (__all_sync(0xffffffffu, bmax < 0x800000u)) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = iq_fast(s2[k], fq);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = iq_dec(s2[k], q);
+      }
     } else if (!raw) {
       // chunks stored uncompressed are copied out as stored: original floats
       // for storage decode (d_server_encode.h:234-249), request bins for

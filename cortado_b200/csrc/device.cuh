@@ -187,6 +187,41 @@ __device__ __forceinline__ uint32_t iq_dec(uint32_t enc, const Quant& q) {
   return enc ? dec : 0u;
 }
 
+// Float forms for lossy words.  A float below the bound's lossless threshold
+// (|x| < 2^(thr_e - 127)) has SQ bin trunc(x * 2^(126 - eb_e)) and CQ bin
+// x * 2^(126 - eb_e) rounded half away from zero; a bin below 2^23 in
+// magnitude dequantizes to bin * 2^(eb_e - 126).  The scaling by a power of
+// two is exact and |x| * scale < 2^23, so one multiply (or fused multiply-add
+// with +-0.5) and a truncating conversion give the integer formulas' results;
+// floats below 2^(eb_e - 127) have CQ bin 0 (their shift is 25 or more, and
+// there the +0.5 could round the sum up to 1).  They run on the FMA and
+// conversion units instead of the integer ALU.
+struct FastQ {
+  float sc;           // 2^(126 - eb_e)
+  float dsc;          // 2^(eb_e - 126)
+  uint32_t thr_bits;  // lossless threshold, as float bits (thr_e << 23)
+  uint32_t lo_bits;   // 2^(eb_e - 127), as float bits
+};
+__device__ __forceinline__ FastQ make_fastq(int eb_e) {
+  FastQ f;
+  f.sc = __uint_as_float((uint32_t)(253 - eb_e) << 23);
+  f.dsc = __uint_as_float((uint32_t)(eb_e + 1) << 23);
+  f.thr_bits = (uint32_t)(eb_e + 24) << 23;
+  f.lo_bits = (uint32_t)eb_e << 23;
+  return f;
+}
+__device__ __forceinline__ uint32_t sq_fast(uint32_t v, const FastQ& f) {
+  return (uint32_t)__float2int_rz(__fmul_rn(__uint_as_float(v), f.sc));
+}
+__device__ __forceinline__ uint32_t cq_fast(uint32_t v, const FastQ& f) {
+  const uint32_t r =
+      (uint32_t)__float2int_rz(__fmaf_rn(__uint_as_float(v), f.sc, __uint_as_float((v & 0x80000000u) | 0x3f000000u)));
+  return (v & 0x7fffffffu) < f.lo_bits ? 0u : r;
+}
+__device__ __forceinline__ uint32_t iq_fast(uint32_t enc, const FastQ& f) {
+  return __float_as_uint(__fmul_rn(__int2float_rn((int)enc), f.dsc));
+}
+
 // ---------------------------------------------------------------- BIT_4
 // The reference's BIT_4 warp butterfly (include/components/d_BIT_4.h:41-92)
 // maps input word i, bit b of a 32-word group to output plane 31-b, bit 31-i:
