@@ -610,7 +610,39 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
   const uint32_t zoff = block_scan_excl(nz, sm.scan_b, NZ);
   if (NZ != zbase) ok = false;
   if (!ok) latch(sy.status, DST_CORRUPT);
-  // ZE decode: scatter the non-zero bytes back into the 32 words.
+  // ZE decode: scatter the non-zero bytes back into the 32 words.  A warp
+  // whose threads each hold at most 4 non-zero words expands just those (kept
+  // in registers until every payload byte has been read) into zero-filled
+  // rows; a denser warp expands all 32 words.
+  uint32_t wm = ok ? (nz_nibbles8(M[0]) | (nz_nibbles8(M[1]) << 8) | (nz_nibbles8(M[2]) << 16) |
+                      (nz_nibbles8(M[3]) << 24))
+                   : 0u;
+  if (__all_sync(0xffffffffu, __popc(wm) <= 4)) {
+    uint32_t kv[4], xv[4];
+    uint32_t p = (uint32_t)d + zoff;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      kv[i] = 32;
+      xv[i] = 0;
+      if (wm) {
+        const uint32_t k = __ffs(wm) - 1;
+        wm &= wm - 1;
+        const uint32_t mk = nibble_at(M, k);
+        const uint32_t lo = P[p >> 2], hi = P[(p >> 2) + 1];
+        xv[i] = __byte_perm(__funnelshift_r(lo, hi, 8 * (p & 3)), 0u, expand_sel(mk));
+        kv[i] = k;
+        p += __popc(mk);
+      }
+    }
+    if (inplace) __syncthreads();  // every payload byte has been read
+    uint4* row = reinterpret_cast<uint4*>(plane + 32 * tid);
+#pragma unroll
+    for (int u = 0; u < 8; u++) row[u ^ (tid & 7)] = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (kv[i] < 32) plane[swz(32 * tid + kv[i])] = xv[i];
+    __syncthreads();
+  } else {
   uint32_t q[32];
   if (!ok || (M[0] | M[1] | M[2] | M[3]) == 0) {
 #pragma unroll
@@ -632,6 +664,7 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
   if (inplace) __syncthreads();  // every payload byte has been read
   row_store(plane, tid, q);
   __syncthreads();
+  }
   planes_to_words<FULL>(sm, plane, nw, v);
 }
 
