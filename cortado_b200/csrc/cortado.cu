@@ -469,6 +469,16 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
   flush_pending(sm, src, s ^ 1, B, raw_word);
 }
 
+// Rebuilds a raw chunk's requantized words from the plane buffer into the
+// staging buffer (out of line: only chunks that do not compress take it, and
+// the re-encoders' loop is large enough to stall on instruction fetch).
+__device__ __noinline__ void raw_rebuild(Ctl& sm, const uint32_t* X, int nw, uint32_t* Yw) {
+  uint32_t w[32];
+  if (nw == CW) planes_to_words<true>(sm, X, nw, w);
+  else planes_to_words<false>(sm, X, nw, w);
+  row_store(Yw, threadIdx.x, w);
+}
+
 // init_send / resi_send (d_s2c_encode_kernel, d_residual_encode_kernel):
 // decode the stored chunk, requantize or form the residual, encode.  The
 // payload arrives in buffer 0 and is expanded in place; after the
@@ -579,9 +589,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       }
       if (sm.pend[s].raw) {
         // the requantized words, rebuilt from the plane buffer, are the payload
-        if (nw == CW) planes_to_words<true>(sm, X, nw, v);
-        else planes_to_words_partial(sm, X, nw, v);
-        row_store(Yw, tid, v);
+        raw_rebuild(sm, X, nw, Yw);
       }
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;

@@ -679,13 +679,6 @@ __device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint3
   encode_stage<false>(sm, sy, w, plane, st, c, nw, item, pend, NoHook{});
 }
 
-__device__ __noinline__ void planes_to_words_partial(Ctl& sm, const uint32_t* plane, int nw, uint32_t* v) {
-  uint32_t w[32];
-  planes_to_words<false>(sm, plane, nw, w);
-#pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = w[k];
-}
-
 template <typename Side>
 __device__ __noinline__ void decode_core_partial(Ctl& sm, const Sync& sy, const StageMeta& m, uint32_t* P,
                                                  uint32_t* plane, uint32_t* v, bool& raw_out, Side side) {
