@@ -368,14 +368,17 @@ def bench_batched(codec, dev, n_fields=64, seed=3, max_mb=256, bounds=("1e-1", "
             **res, "speedup": res["plain"]["ms"] / res["batched"]["ms"]}
 
 
-def bench_serving(dev, n_fields=32, n_requests=400, rate_hz=2000.0, seed=5, max_mb=512):
+def bench_serving(dev, n_fields=32, n_requests=400, rates=(2000.0, 8000.0, 32000.0, None), seed=5, max_mb=512):
     """Serving configuration: resident stored fields (4..max_mb MiB, mixed
     generators), Poisson arrivals (60% init at NOA 1e-1..1e-3, 40% residual 1-3
-    decades finer); continuous batching vs the plain per-request pipeline."""
+    decades finer); continuous batching vs the plain per-request pipeline at a
+    swept arrival rate.  The same request sequence is replayed at every rate
+    (arrival times scaled); rate None queues every request at the start, so
+    the aggregate GB/s there is each pipeline's capacity."""
     from cortado_b200 import fields, storage
     from cortado_b200.serve import Server, poisson_trace
     rng = np.random.Generator(np.random.PCG64(seed))
-    srv = Server(dev.index, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3)
+    srv = Server(dev.index, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3, max_batch=16)
     kinds = ("sinusoid", "grf", "white")
     ranges = {}
     for i in range(n_fields):
@@ -384,27 +387,35 @@ def bench_serving(dev, n_fields=32, n_requests=400, rate_hz=2000.0, seed=5, max_
         r = float(x.max() - x.min())
         ranges[f"f{i}"] = r
         srv.add_field(f"f{i}", x, [float(storage.noa_scale(e, r)) for e in (1e-1, 1e-3, 1e-5, 1e-7)])
-    trace = poisson_trace(rng, srv.fields, n_requests, rate_hz, n_clients=16, ranges=ranges)
+    trace = poisson_trace(rng, srv.fields, n_requests, 1.0, n_clients=16, ranges=ranges)
+    unit_arrivals = [r.arrival for r in trace]  # at one request per second
     # Client reconstructions are allocated up front (a server does that when a
-    # client opens a field); each mode serves the trace once untimed, so the
-    # allocator holds its output streams, then once measured, from fresh
-    # client progress on the same buffers.
+    # client opens a field); each mode serves the trace once untimed at the
+    # backlog point (the most requests in flight), so the allocator holds its
+    # output streams, then once measured per rate, from fresh client progress
+    # on the same buffers.
     srv.prepare(trace)
 
-    def once(fn):
+    def once(fn, rate):
         srv.reset_clients(free=False)
-        for r in trace:
+        for r, u in zip(trace, unit_arrivals):
             r.done = -1.0
+            r.arrival = u / rate if rate else 0.0
         return fn(trace)[0]
 
-    once(srv.run)
-    served = once(srv.run)
-    once(srv.run_plain)
-    plain = once(srv.run_plain)
+    once(srv.run, None)
+    once(srv.run_plain, None)
+    sweep = []
+    for rate in rates:
+        served = once(srv.run, rate)
+        plain = once(srv.run_plain, rate)
+        sweep.append({"rate_hz": rate if rate else "backlog", "served": served, "plain": plain,
+                      "speedup": served["orig_GBps"] / plain["orig_GBps"] if plain["orig_GBps"] else None})
     srv.close()
-    return {"workload": f"{n_fields} resident fields 4-{max_mb} MiB, {n_requests} requests, Poisson {rate_hz:g}/s, "
-                        "60% init / 40% residual", "served": served, "plain": plain,
-            "speedup": served["orig_GBps"] / plain["orig_GBps"] if plain["orig_GBps"] else None}
+    cap = sweep[-1]
+    return {"workload": f"{n_fields} resident fields 4-{max_mb} MiB, {n_requests} requests, Poisson arrivals at "
+                        f"{[s['rate_hz'] for s in sweep]} per s, 60% init / 40% residual",
+            "sweep": sweep, "served": cap["served"], "plain": cap["plain"], "speedup": cap["speedup"]}
 
 
 def load_traffic():
@@ -506,7 +517,8 @@ def main():
                      "per_kernel_frac": {k: alg[k] / (op_ms[k] * 1e-3) * 1e-9 / peak for k in alg}},
         "e2e": {"value": world * n * 1e-9 / (r["e2e_ms"] * 1e-3), "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
-        "gpu_launches": args.steps * (len(OPS)),
+        # one kernel per operation, two for the NOA range (min/max, hand-over)
+        "gpu_launches": args.steps * (len(OPS) + 1),
         "abs_mode": {"bounds_abs": {"store": ABS_STORE, "init": ABS_SRC, "resi": [ABS_SRC, ABS_DST]},
                      "value": job_gbs(n, world, r["abs"]["ms"]), "ms_per_step": r["abs"]["ms"],
                      "bounds_verified": r["abs"]["ok"],

@@ -10,14 +10,18 @@ client's current reconstruction resident in HBM.  Requests:
   reconstruction in place.
 
 Requests arrive over time (``Request.arrival`` in seconds from the start).
-Each loop iteration admits every arrived request that fits. Admission needs a
-free slot (``max_inflight``), device memory under ``mem_cap_bytes`` for its
-output stream, and no other request of the same client in flight (a client's
-steps are ordered).  The admitted requests are grouped by operation and run as
-batched launches (``cortado_batch``: one persistent launch per operation for
-the whole group) on one of ``n_streams`` CUDA streams.  Admission does not
-wait for earlier batches: a new batch starts on the next stream while others
-are still on the GPU, and completions are polled with CUDA events.  A request's
+Each loop iteration admits arrived requests, in arrival order, up to
+``max_batch`` per batch.  Admission needs a free slot (``max_inflight``),
+device memory under ``mem_cap_bytes`` for its output stream, and no earlier
+request of the same client on the same field still running or waiting (a
+client's steps are ordered); a request held back for that reason does not hold
+back other clients' requests.  The admitted requests are grouped by operation
+and run as batched launches (``cortado_batch``: one persistent launch per
+operation for the whole group) on one of ``n_streams`` CUDA streams.
+Admission does not wait for earlier batches: a new batch starts on the next
+stream while others are still on the GPU (several batches in flight keep the
+GPU busy while the host assembles the next one), and completions are polled
+with CUDA events.  A request's
 latency is its completion time (the host clock when its batch's event is seen
 complete) minus its arrival.
 
@@ -62,12 +66,13 @@ class Field:
 
 
 class Server:
-    def __init__(self, device=0, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3):
+    def __init__(self, device=0, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3, max_batch=16):
         self.dev = torch.device("cuda", device)
         self.codecs = [Codec(device) for _ in range(n_streams)]
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
         self.mem_cap = mem_cap_bytes
         self.max_inflight = max_inflight
+        self.max_batch = max_batch
         self.fields: dict[str, Field] = {}
         self.clients: dict[tuple, dict] = {}   # (client, field) -> {"recon": tensor, "bound": float}
         self.mem_used = 0
@@ -155,12 +160,13 @@ class Server:
         """Serves the trace with continuous batching; returns stats."""
         pending = sorted(requests, key=lambda r: r.arrival)
         inflight = []          # (event, reqs, outs, sizes, bytes, stream index)
+        waiting = []           # arrived, not yet admitted, in arrival order
         busy_clients = set()
         outputs = {}
         t0 = time.perf_counter()
         k = 0
         i = 0
-        while i < len(pending) or inflight:
+        while i < len(pending) or waiting or inflight:
             now = time.perf_counter() - t0
             # completions
             still = []
@@ -178,28 +184,42 @@ class Server:
                 else:
                     still.append(item)
             inflight = still
-            # admission
-            batch, nbytes = [], 0
-            room = self.max_inflight - sum(len(x[1]) for x in inflight)
-            while i < len(pending) and pending[i].arrival <= now and len(batch) < room:
-                r = pending[i]
-                if (r.client, r.field) in busy_clients or any((b.client, b.field) == (r.client, r.field) for b in batch):
-                    break  # keep arrival order; this client's previous step is still running
-                need = max_stream_bytes(self.fields[r.field].n_bytes)
-                if self.mem_used + nbytes + need > self.mem_cap:
-                    break
-                batch.append(r)
-                nbytes += need
+            # admission: in arrival order, except that a request whose client
+            # (on that field) has an earlier step running or waiting is passed
+            # over, together with that client's later requests
+            while i < len(pending) and pending[i].arrival <= now:
+                waiting.append(pending[i])
                 i += 1
+            batch, nbytes = [], 0
+            room = min(self.max_batch, self.max_inflight - sum(len(x[1]) for x in inflight))
+            if room > 0 and waiting:
+                held, keep = set(), []
+                for j, r in enumerate(waiting):
+                    if len(batch) >= room:
+                        keep.extend(waiting[j:])
+                        break
+                    key = (r.client, r.field)
+                    if key in busy_clients or key in held:
+                        held.add(key)
+                        keep.append(r)
+                        continue
+                    need = max_stream_bytes(self.fields[r.field].n_bytes)
+                    if self.mem_used + nbytes + need > self.mem_cap:
+                        keep.extend(waiting[j:])
+                        break
+                    batch.append(r)
+                    busy_clients.add(key)
+                    nbytes += need
+                waiting = keep
             if batch:
                 self.mem_used += nbytes
-                for r in batch:
-                    busy_clients.add((r.client, r.field))
                 ev, outs, sizes = self._launch(k, batch)
                 inflight.append((ev, batch, outs, sizes, nbytes, k))
                 k = (k + 1) % len(self.streams)
             elif inflight:
                 time.sleep(20e-6)
+            elif waiting:
+                raise RuntimeError(f"request {waiting[0].rid} needs more than the {self.mem_cap}-byte memory cap")
             elif i < len(pending):
                 time.sleep(max(0.0, min(1e-3, pending[i].arrival - (time.perf_counter() - t0))))
         for c, s in zip(self.codecs, self.streams):

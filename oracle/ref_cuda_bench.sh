@@ -10,7 +10,7 @@
 set -u
 HERE="$(cd "$(dirname "$0")" && pwd)"
 ROOT="$(cd "$HERE/.." && pwd)"
-OUT="${1:-$ROOT/gpurun_out/refbench}"
+OUT="${1:-${TMPDIR:-/tmp}/cortado_refbench}"
 mkdir -p "$OUT"
 F="${TMPDIR:-/tmp}/cortado_field_512.f32"
 python3 -c "

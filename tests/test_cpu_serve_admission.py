@@ -1,0 +1,107 @@
+"""Admission logic of the continuous-batching server (Server.run), on the CPU:
+the GPU launches are replaced by fakes whose completion events report done
+after a few polls.  Checked: a client's steps on a field start only after its
+previous step finished and in arrival order; batches hold at most max_batch
+requests; at most max_inflight requests are in flight; the memory cap holds;
+a client held back by its own running step does not hold back other clients;
+a request larger than the memory cap is an error, not a hang."""
+import numpy as np
+import pytest
+import torch
+
+from cortado_b200 import serve
+from cortado_b200.ops import max_stream_bytes
+
+
+class _Event:
+    def __init__(self, polls):
+        self.polls = polls
+
+    def query(self):
+        self.polls -= 1
+        return self.polls < 0
+
+
+class _Codec:
+    def sync(self, stream=None):
+        pass
+
+
+def _server(sizes, max_inflight, max_batch, mem_cap, polls=3):
+    srv = serve.Server.__new__(serve.Server)
+    srv.dev = torch.device("cpu")
+    srv.codecs = [_Codec() for _ in range(3)]
+    srv.streams = [None] * 3
+    srv.mem_cap = mem_cap
+    srv.max_inflight = max_inflight
+    srv.max_batch = max_batch
+    srv.fields = {name: serve.Field(name, torch.zeros(n // 4), [1.0]) for name, n in sizes.items()}
+    srv.clients = {}
+    srv.mem_used = 0
+    launches, launched = [], []
+
+    def fake_launch(k, reqs):
+        launched.extend(reqs)
+        launches.append({"stream": k, "rids": [r.rid for r in reqs],
+                         "inflight": sum(1 for r in launched if r.done < 0),
+                         "mem_used": srv.mem_used,
+                         "prev_done": [all(p.done >= 0 for p in launched[:-len(reqs)]
+                                           if (p.client, p.field) == (r.client, r.field)) for r in reqs]})
+        return _Event(polls), {r.rid: None for r in reqs}, None
+
+    srv._launch = fake_launch
+    return srv, launches
+
+
+def _trace(rng, names, n, n_clients, rate_hz):
+    reqs, t = [], 0.0
+    for rid in range(n):
+        if rate_hz:
+            t += rng.exponential(1.0 / rate_hz)
+        reqs.append(serve.Request(rid, "init" if rng.random() < 0.6 else "resi", int(rng.integers(n_clients)),
+                                  names[int(rng.integers(len(names)))], 1e-3, t))
+    return reqs
+
+
+@pytest.mark.parametrize("rate_hz", [None, 5e4])
+@pytest.mark.parametrize("max_batch,max_inflight", [(1, 4), (4, 8), (16, 64)])
+def test_admission_invariants(rate_hz, max_batch, max_inflight):
+    rng = np.random.Generator(np.random.PCG64(3))
+    sizes = {f"f{i}": int(rng.integers(1, 64)) << 16 for i in range(6)}
+    cap = 5 * max(max_stream_bytes(n) for n in sizes.values())
+    srv, launches = _server(sizes, max_inflight, max_batch, cap)
+    trace = _trace(rng, sorted(sizes), 120, 3, rate_hz)
+    stats, _ = srv.run(trace)
+    assert stats["requests"] == len(trace)
+    assert all(r.done >= r.arrival for r in trace)
+    order = [rid for b in launches for rid in b["rids"]]
+    assert sorted(order) == list(range(len(trace)))
+    for b in launches:
+        assert 1 <= len(b["rids"]) <= max_batch
+        assert b["inflight"] <= max_inflight
+        assert b["mem_used"] <= cap
+        assert all(b["prev_done"])
+    pos = {rid: i for i, rid in enumerate(order)}
+    by_key = {}
+    for r in trace:
+        by_key.setdefault((r.client, r.field), []).append(r.rid)
+    for rids in by_key.values():
+        assert [pos[x] for x in rids] == sorted(pos[x] for x in rids)
+    assert srv.mem_used == 0
+
+
+def test_held_client_does_not_block_others():
+    sizes = {"a": 1 << 20, "b": 1 << 20}
+    srv, launches = _server(sizes, 16, 16, 10**12)
+    R = serve.Request
+    trace = [R(0, "init", 0, "a", 1e-3, 0.0), R(1, "resi", 0, "a", 1e-4, 0.0), R(2, "init", 1, "a", 1e-3, 0.0),
+             R(3, "init", 0, "b", 1e-3, 0.0), R(4, "resi", 0, "a", 1e-5, 0.0), R(5, "init", 2, "b", 1e-3, 0.0)]
+    srv.run(trace)
+    assert launches[0]["rids"] == [0, 2, 3, 5]
+    assert [b["rids"] for b in launches[1:]] == [[1], [4]]
+
+
+def test_request_over_memory_cap_raises():
+    srv, _ = _server({"a": 1 << 20}, 16, 16, 1 << 10)
+    with pytest.raises(RuntimeError, match="memory cap"):
+        srv.run([serve.Request(0, "init", 0, "a", 1e-3, 0.0)])

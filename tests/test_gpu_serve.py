@@ -2,7 +2,8 @@
 stream) and every client's final reconstruction are identical when the trace
 is served batched and overlapped (Server.run) and when each request runs alone
 through the plain per-request pipeline (Server.run_plain); p50/p99 latencies
-are reported."""
+are reported.  Served at a Poisson rate and as a backlog (every request queued
+at the start, small batches, so admission passes held-back clients)."""
 import numpy as np
 import pytest
 import torch
@@ -13,9 +14,9 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _server(dev_index):
+def _server(dev_index, max_batch=16):
     from cortado_b200.serve import Server
-    srv = Server(dev_index, mem_cap_bytes=4 * 10**9, max_inflight=16, n_streams=3)
+    srv = Server(dev_index, mem_cap_bytes=4 * 10**9, max_inflight=16, n_streams=3, max_batch=max_batch)
     gens = {"a": fields.mixed_field(262144, "sinusoid", 1), "b": fields.mixed_field(1000000, "grf", 2),
             "c": fields.mixed_field(500001, "white", 3)}
     ranges = {}
@@ -27,11 +28,15 @@ def _server(dev_index):
     return srv, ranges
 
 
-def test_served_results_equal_alone(cuda_device):
+@pytest.mark.parametrize("backlog,max_batch", [(False, 16), (True, 4)])
+def test_served_results_equal_alone(cuda_device, backlog, max_batch):
     from cortado_b200.serve import poisson_trace
-    srv, ranges = _server(cuda_device.index)
+    srv, ranges = _server(cuda_device.index, max_batch)
     rng = np.random.Generator(np.random.PCG64(11))
     trace = poisson_trace(rng, srv.fields, 60, rate_hz=20000.0, n_clients=4, ranges=ranges)
+    if backlog:  # every request queued at the start: batches of 4, clients passing each other
+        for r in trace:
+            r.arrival = 0.0
     stats_b, out_b = srv.run(trace, keep_outputs=True)
     recon_b = {k: v["recon"].clone() for k, v in srv.clients.items()}
     bounds_b = {k: v["bound"] for k, v in srv.clients.items()}
