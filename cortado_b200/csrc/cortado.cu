@@ -390,6 +390,35 @@ __device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, co
   }
 }
 
+// The integer quantizer forms for the words (bit k of m) that the encoders'
+// fast forms cannot take.  The choice is per word, so one outlier no longer
+// sends its warp's 1024 words down the slow path.  Out of line: such words are
+// rare (lossless words, inf, NaN, raw chunks), and inlining the slow forms 32
+// times over made the loops large enough to stall on instruction fetch.
+__device__ __noinline__ void sq_words(uint32_t (&v)[32], uint32_t m, Quant q) {
+  for (; m; m &= m - 1) {
+    const int k = __ffs(m) - 1;
+    v[k] = sq_enc(v[k], q);
+  }
+}
+// Requantization through floats (d_s2c.h:132-137, d_RESI_4.h:57-76): the
+// stored bin (or, for a raw chunk, the float itself) -> float (iSQ) -> request
+// bin (CQ), or residual = destination bin minus the request bin requantized
+// to the destination bound.
+template <int OP>
+__device__ __noinline__ void requant_words(uint32_t (&v)[32], uint32_t m, bool raw, Quant qs, Quant q1, Quant q2) {
+  for (; m; m &= m - 1) {
+    const int k = __ffs(m) - 1;
+    const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+    if (OP == OP_S2C) {
+      v[k] = cq_enc(x, q1);
+    } else {
+      const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
+      v[k] = cq_enc(x, q2) - src_req;
+    }
+  }
+}
+
 // store (d_server_encode_kernel): floats -> SQ -> encode.  A chunk arrives in
 // buffer 0, which becomes its plane buffer; its compacted payload goes to
 // buffer 1 once the previous chunk's payload has been flushed from there (that
@@ -439,18 +468,17 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
     row_load(A, tid, v);
     const Quant q1 = A_.q1;
     {
-      // the float form when every word of the warp is below the lossless threshold
+      // the float form for words below the lossless threshold; the others
+      // (lossless words, inf, NaN) out of line
       const FastQ fq = make_fastq(q1.eb_e);
-      uint32_t amax = 0;
+      uint32_t slow = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) amax = max(amax, v[k] & 0x7fffffffu);
-      if (__all_sync(0xffffffffu, amax < fq.thr_bits)) {
-#pragma unroll
-        for (int k = 0; k < 32; k++) v[k] = sq_fast(v[k], fq);
-      } else {
-#pragma unroll
-        for (int k = 0; k < 32; k++) v[k] = sq_enc(v[k], q1);
+      for (int k = 0; k < 32; k++) {
+        const bool ok = (v[k] & 0x7fffffffu) < fq.thr_bits;
+        slow |= (ok ? 0u : 1u) << k;
+        v[k] = ok ? sq_fast(v[k], fq) : v[k];
       }
+      if (slow) sq_words(v, slow, q1);
     }
     auto flush_prev = [&]() {
       flush_pending(sm, src, s ^ 1, B, raw_word);
@@ -548,37 +576,28 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       const int k1 = q1.eb_e - qs.eb_e;
       const int k2 = (OP == OP_RESI) ? q2.eb_e - qs.eb_e : 0;
       const int dd = (OP == OP_RESI) ? q1.eb_e - q2.eb_e : 0;
+      // Words the shift form cannot take (lossless stored words, magnitudes
+      // at or above amax, every word of a chunk stored raw or of a bound
+      // order it does not cover) go through the float path out of line.
+      // (amax = 0 when the shift form does not apply: no word qualifies and
+      // every word keeps its stored bin for the float path.)
       const bool shift_ok = !raw && k1 >= 0 && k2 >= 0 && dd >= 0;
-      const uint32_t amax =
-          (OP == OP_RESI && k2 == 0 && k1 >= 1 && k1 <= 23) ? 0x800000u - (1u << (k1 - 1)) : 0x800000u;
-      uint32_t big = 0;
+      const uint32_t amax = !shift_ok ? 0u
+                            : (OP == OP_RESI && k2 == 0 && k1 >= 1 && k1 <= 23) ? 0x800000u - (1u << (k1 - 1))
+                                                                                 : 0x800000u;
+      const uint32_t h1 = shl_clamp(1u, (uint32_t)(k1 - 1)), h2 = shl_clamp(1u, (uint32_t)(k2 - 1));
+      uint32_t slow = 0;
 #pragma unroll
       for (int k = 0; k < 32; k++) {
         const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
-        big = max(big, (v[k] ^ neg) - neg);
+        const uint32_t a = (v[k] ^ neg) - neg;
+        const uint32_t m1 = shr_clamp(a + h1, (uint32_t)k1);
+        const uint32_t r = (OP == OP_S2C) ? m1 : shr_clamp(a + h2, (uint32_t)k2) - shl_clamp(m1, (uint32_t)dd);
+        const bool ok = a < amax;
+        slow |= (ok ? 0u : 1u) << k;
+        v[k] = ok ? (r ^ neg) - neg : v[k];
       }
-      if (__all_sync(0xffffffffu, shift_ok && big < amax)) {
-        const uint32_t h1 = shl_clamp(1u, (uint32_t)(k1 - 1)), h2 = shl_clamp(1u, (uint32_t)(k2 - 1));
-#pragma unroll
-        for (int k = 0; k < 32; k++) {
-          const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
-          const uint32_t a = (v[k] ^ neg) - neg;
-          const uint32_t m1 = shr_clamp(a + h1, (uint32_t)k1);
-          const uint32_t r = (OP == OP_S2C) ? m1 : shr_clamp(a + h2, (uint32_t)k2) - shl_clamp(m1, (uint32_t)dd);
-          v[k] = (r ^ neg) - neg;
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 32; k++) {
-          const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
-          if (OP == OP_S2C) {
-            v[k] = cq_enc(x, q1);
-          } else {
-            const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
-            v[k] = cq_enc(x, q2) - src_req;
-          }
-        }
-      }
+      if (slow) requant_words<OP>(v, slow, raw, qs, q1, q2);
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
       if (nw == CW) {
         encode_stage<true>(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s], flush_prev);
@@ -673,7 +692,9 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
       }
       uint32_t s2[32];
       row_load(P, tid, s2);
-      // float forms when every word of the warp is lossy (client float, then sum)
+      // float forms when every word of the warp is lossy (client float, then
+      // sum).  A per-word choice with the integer forms out of line, as in the
+      // encoders, measured 12% slower here: both arrays then live in memory.
       const FastQ fq = make_fastq(m.eb_e);
       uint32_t amax = 0;
 #pragma unroll

@@ -139,6 +139,34 @@ def test_all_ops_match_oracle(codec, nbytes, kind):
         assert np.array_equal(bits(fin_g), bits(fin_o)), ("resi_recv", eb_noa)
 
 
+@pytest.mark.parametrize("req,dst", [(10.0, 2.0), (0.5, 0.25), (0.25, 0.1), (4.0, 1.0), (1.0, 4.0), (3.0, 0.3), (1.0, 1.0)])
+def test_requant_bound_orders_match_oracle(codec, req, dst):
+    """init_send / resi_send with request and destination bounds above, equal
+    to and below the stored bound (multiples of it), on a field whose warps mix
+    lossy words with lossless outliers and infinities: the encoders choose
+    between the fast forms and the integer forms word by word."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    nw = 8 * 4096 + 300
+    x = rng.normal(0, 1, nw).astype(np.float32)
+    idx = rng.choice(nw, nw // 500, replace=False)
+    x[idx] = (rng.choice([-1.0, 1.0], idx.size) * rng.uniform(1e5, 1e7, idx.size)).astype(np.float32)
+    x[idx[:2]] = [np.inf, -np.inf]
+    eb = 1e-3
+    stor_o = O.store_encode(x, eb)
+    stor_g = codec.store(torch.from_numpy(x).cuda(), eb)
+    assert u8(stor_g) == stor_o
+    init_o = O.init_send(stor_o, eb * req)
+    init_g = codec.init_send(stor_g, eb * req)
+    assert u8(init_g) == init_o
+    cl_o = O.init_recv(init_o)
+    cl_g = codec.init_recv(init_g)
+    assert np.array_equal(bits(cl_g), bits(cl_o))
+    resi_o = O.resi_send(stor_o, eb * req, eb * dst)
+    resi_g = codec.resi_send(stor_g, eb * req, eb * dst)
+    assert u8(resi_g) == resi_o
+    assert np.array_equal(bits(codec.resi_recv(cl_g, resi_g)), bits(O.resi_recv(cl_o, resi_o)))
+
+
 def test_noa_range_matches(codec):
     for seed in range(3):
         x = fields.white(100003 * 4 // 4, seed).numpy() * (seed + 1)
