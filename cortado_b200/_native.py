@@ -38,6 +38,7 @@ SIGNATURES = {
     "cortado_batch": (_int, [_vp, _int, _vp, _int, _vp]),
     "cortado_verify_bound": (_int, [_vp, _vp, _vp, _i64, _f32, _vp, _vp]),
     "cortado_set_launch_ctas": (_int, [_vp, _int, _int]),
+    "cortado_reserve": (_int, [_vp, _i64, _int]),
 }
 
 OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5}

@@ -1025,6 +1025,28 @@ cortado_status ensure_flags(cortado_ctx* ctx, int64_t chunks, cudaStream_t st) {
   return CORTADO_OK;
 }
 
+// Batch item tables: ITEM_SLOTS tables of at least n_items entries each.
+// Growing waits for every launch that reads a table.
+cortado_status ensure_items(cortado_ctx* ctx, int n_items) {
+  constexpr int SLOTS = cortado_ctx::ITEM_SLOTS;
+  if (n_items <= ctx->items_cap) return CORTADO_OK;
+  for (cudaEvent_t ev : ctx->items_done) cudaEventSynchronize(ev);  // every table is free
+  cudaFree(ctx->d_items);
+  cudaFreeHost(ctx->h_items);
+  ctx->d_items = nullptr;
+  ctx->h_items = nullptr;
+  int cap = 64;
+  while (cap < n_items) cap *= 2;
+  cudaError_t e = cudaMalloc(&ctx->d_items, sizeof(BatchItem) * cap * SLOTS);
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_items, sizeof(BatchItem) * cap * SLOTS);
+  if (e != cudaSuccess) {
+    ctx->items_cap = 0;
+    return from_cuda(e);
+  }
+  ctx->items_cap = cap;
+  return CORTADO_OK;
+}
+
 Sync next_sync(cortado_ctx* ctx, cudaStream_t) {
   Sync s;
   s.flags = ctx->flags;
@@ -1152,6 +1174,14 @@ cortado_status cortado_set_timeout(cortado_ctx* ctx, uint64_t timeout_ns) {
   if (!ctx || timeout_ns == 0) return CORTADO_ERR_INVALID_ARG;
   ctx->timeout_ns = timeout_ns;
   return CORTADO_OK;
+}
+
+cortado_status cortado_reserve(cortado_ctx* ctx, int64_t chunks, int items) {
+  if (!ctx || chunks < 0 || items < 0) return CORTADO_ERR_INVALID_ARG;
+  cortado_status s = ensure_flags(ctx, chunks, 0);
+  if (s) return s;
+  if ((s = ensure_items(ctx, items))) return s;
+  return from_cuda(cudaStreamSynchronize(0));
 }
 
 cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas_per_sm) {
@@ -1372,19 +1402,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   cortado_status s = ensure_flags(ctx, total, st);
   if (s) return s;
   constexpr int SLOTS = cortado_ctx::ITEM_SLOTS;
-  if (n_items > ctx->items_cap) {
-    for (cudaEvent_t ev : ctx->items_done) cudaEventSynchronize(ev);  // every table is free
-    cudaFree(ctx->d_items);
-    cudaFreeHost(ctx->h_items);
-    ctx->d_items = nullptr;
-    ctx->h_items = nullptr;
-    int cap = 64;
-    while (cap < n_items) cap *= 2;
-    cudaError_t e = cudaMalloc(&ctx->d_items, sizeof(BatchItem) * cap * SLOTS);
-    if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_items, sizeof(BatchItem) * cap * SLOTS);
-    if (e != cudaSuccess) { ctx->items_cap = 0; return from_cuda(e); }
-    ctx->items_cap = cap;
-  }
+  if ((s = ensure_items(ctx, n_items))) return s;
   const int slot = ctx->items_slot;
   ctx->items_slot = (slot + 1) % SLOTS;
   cudaEventSynchronize(ctx->items_done[slot]);  // the launch that last read this slot has ended

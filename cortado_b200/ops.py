@@ -86,6 +86,12 @@ class Codec:
     def set_timeout(self, seconds: float):
         check(self._L.cortado_set_timeout(self._h, int(seconds * 1e9)), "set_timeout")
 
+    def reserve(self, chunks: int, items: int = 0):
+        """Sizes the scratch for calls of up to `chunks` chunks (all items of a
+        batched call together) and `items` batch items, so that no later call
+        allocates device memory."""
+        check(self._L.cortado_reserve(self._h, int(chunks), int(items)), "reserve")
+
     def set_launch_ctas(self, op: str, ctas_per_sm: int):
         """Persistent-grid size of one operation (0 = occupancy limit)."""
         check(self._L.cortado_set_launch_ctas(self._h, _native.OPS[op], int(ctas_per_sm)), "set_launch_ctas")

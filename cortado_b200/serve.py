@@ -76,6 +76,12 @@ class Server:
         self.fields: dict[str, Field] = {}
         self.clients: dict[tuple, dict] = {}   # (client, field) -> {"recon": tensor, "bound": float}
         self.mem_used = 0
+        # Output stream buffers, per field (each field's capacity is fixed),
+        # reused once the batch that held one is seen complete: after a
+        # warm-up the loop allocates no device memory.  (Allocating per request
+        # through the caching allocator, across several streams, sometimes
+        # fell back to a fresh cudaMalloc, which stalls the device.)
+        self._free_out: dict[str, list[torch.Tensor]] = {}
 
     # ---------------------------------------------------------------- storage
     def add_field(self, name, x, store_bounds_abs):
@@ -97,6 +103,12 @@ class Server:
             self.clients[key] = st
             self.mem_used += f.n_bytes
         return st
+
+    def _out_buffer(self, f: Field) -> torch.Tensor:
+        free = self._free_out.get(f.name)
+        if free:
+            return free.pop()
+        return torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
 
     def _stored_for(self, f: Field, bound):
         i = storage.select_stored([storage.f32(e) for e in f.store_bounds], bound)
@@ -120,8 +132,7 @@ class Server:
         for r in inits:
             f = self.fields[r.field]
             st = self._recon(r.client, r.field)
-            with torch.cuda.stream(s):
-                out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
+            out = self._out_buffer(f)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
                                    n_bytes=f.n_bytes, eb1=r.bound))
@@ -138,8 +149,7 @@ class Server:
             st = self._recon(r.client, r.field)
             if st["bound"] is None:
                 raise ValueError(f"request {r.rid}: residual before init")
-            with torch.cuda.stream(s):
-                out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
+            out = self._out_buffer(f)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
                                    n_bytes=f.n_bytes, eb1=st["bound"], eb2=r.bound))
@@ -177,9 +187,11 @@ class Server:
                     for r in reqs:
                         r.done = tdone
                         busy_clients.discard((r.client, r.field))
-                    if keep_outputs:
-                        for r in reqs:
+                    for r in reqs:
+                        if keep_outputs:  # handed to the caller, not reused
                             outputs[r.rid] = outs[r.rid]
+                        else:
+                            self._free_out.setdefault(r.field, []).append(outs[r.rid])
                     self.mem_used -= nbytes
                 else:
                     still.append(item)
@@ -270,10 +282,15 @@ class Server:
 
     def prepare(self, requests: list[Request]):
         """Allocates the reconstruction of every (client, field) the requests
-        touch, as a server does when a client opens a field, so that serving
-        itself allocates only output streams."""
+        touch, as a server does when a client opens a field, and sizes every
+        context's scratch for the largest batch (max_batch requests on the
+        largest field), so that serving itself allocates only output streams."""
         for r in requests:
             self._recon(r.client, r.field)
+        if self.fields:
+            chunks = max(-(-f.n_bytes // 16384) for f in self.fields.values())
+            for c in self.codecs:
+                c.reserve(self.max_batch * chunks, self.max_batch)
         torch.cuda.synchronize(self.dev)
 
     def reset_clients(self, free=True):

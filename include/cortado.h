@@ -158,6 +158,15 @@ typedef struct {
 cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item* items, int n_items,
                              cortado_stream_t stream);
 
+/* Sizes the context's scratch ahead of use: lookback and payload-offset words
+ * for `chunks` chunks in one call (a batched call counts the chunks of all its
+ * items), and batch item tables of `items` entries.  Calls that find their
+ * scratch too small grow it themselves, but growing frees and allocates
+ * device memory, which waits for the device.  A serving loop reserves its
+ * largest batch once at start-up instead.  No counterpart in the reference
+ * (its wrappers allocate per call).  Returns once the scratch is ready. */
+cortado_status cortado_reserve(cortado_ctx* ctx, int64_t chunks, int items);
+
 /* Launch shape of `op` on this context: the persistent grid holds
  * ctas_per_sm CTAs per SM (capped by the kernel's occupancy limit); 0 restores
  * the occupancy limit.  Chosen by the autotuner (cortado_b200/autotune.py);

@@ -38,6 +38,7 @@ def _server(sizes, max_inflight, max_batch, mem_cap, polls=3):
     srv.fields = {name: serve.Field(name, torch.zeros(n // 4), [1.0]) for name, n in sizes.items()}
     srv.clients = {}
     srv.mem_used = 0
+    srv._free_out = {}
     launches, launched = [], []
 
     def fake_launch(k, reqs):

@@ -14,6 +14,16 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
+def _stream_len(buf: torch.Tensor) -> int:
+    """Bytes of the stream at the start of an output buffer: header, size
+    table and payloads (the buffer's capacity beyond that is not written)."""
+    h = buf[:16].cpu().numpy()
+    n = int(h[:8].view(np.int64)[0])
+    chunks = -(-n // 16384)
+    table = buf[16:16 + 2 * chunks].cpu().numpy().view(np.uint16)
+    return 16 + 2 * chunks + int(table.astype(np.int64).sum())
+
+
 def _server(dev_index, max_batch=16):
     from cortado_b200.serve import Server
     srv = Server(dev_index, mem_cap_bytes=4 * 10**9, max_inflight=16, n_streams=3, max_batch=max_batch)
@@ -47,8 +57,8 @@ def test_served_results_equal_alone(cuda_device, backlog, max_batch):
     assert stats_b["requests"] == stats_p["requests"] == len(trace)
     for r in trace:
         a, b = out_b[r.rid], out_p[r.rid]
-        n = int(b.numel())
-        assert torch.equal(a[:n], b), r
+        n = _stream_len(b)
+        assert _stream_len(a) == n and torch.equal(a[:n], b[:n]), r
     for k, v in srv.clients.items():
         assert bounds_b[k] == v["bound"]
         assert torch.equal(recon_b[k].view(torch.int32), v["recon"].view(torch.int32)), k
