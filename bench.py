@@ -121,6 +121,7 @@ class Flow:
     def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream, abs_mode: bool = False):
         from cortado_b200 import ops
         self.c, self.x, self.s, self.abs_mode = codec, x, stream, abs_mode
+        self.stream = stream  # the compute stream, as cortado_b200.pipeline expects
         dev = x.device
         self.n = x.numel() * 4
         cap = ops.max_stream_bytes(self.n)
@@ -205,62 +206,40 @@ def run_gpu(args, rank, world):
 
     # e2e through the C ABI with host buffers: every step copies the field in
     # from pinned host memory and both streams and the final reconstruction
-    # back.  Two flows (own buffers, context and compute stream) alternate;
-    # host->device copies run on their own stream one step ahead, and
-    # device->host copies on another, so a step's copies out overlap the next
-    # step's copy in and compute (the two directions use independent copy
-    # engines).  Events order only the reuse of a flow's buffers.
+    # back, scheduled by cortado_b200.pipeline: two flows (own buffers,
+    # context and compute stream) alternate, copies in run one step ahead on
+    # their own stream and copies out on another, so a step's copies out
+    # overlap the next step's copy in and compute.
+    from cortado_b200.pipeline import Pipeline
     hx = x.cpu().pin_memory()
     s_init, s_resi = int(sizes[1]), int(sizes[3])
     codec2 = ops.Codec(dev.index)
     stream2 = torch.cuda.Stream(dev)
-    cin, cout = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     flows = [Flow(codec, fl.x, stream), Flow(codec2, torch.empty_like(x), stream2)]
     hbufs = [(torch.empty(s_init, dtype=torch.uint8).pin_memory(), torch.empty(s_resi, dtype=torch.uint8).pin_memory(),
               torch.empty(x.numel(), dtype=torch.float32).pin_memory()) for _ in flows]
-    ev_in = [torch.cuda.Event() for _ in flows]    # the flow's field has arrived
-    ev_done = [torch.cuda.Event() for _ in flows]  # the flow's kernels have finished
-    ev_out = [torch.cuda.Event() for _ in flows]   # the flow's outputs have been copied out
-    for k in range(2):
-        ev_done[k].record(flows[k].s)
-        ev_out[k].record(flows[k].s)
 
-    def copy_in(i):
-        k = i % 2
-        cin.wait_event(ev_done[k])  # the previous step of this flow has read its field
-        with torch.cuda.stream(cin):
-            flows[k].x.copy_(hx, non_blocking=True)
-        ev_in[k].record(cin)
+    def load(i, f, s):
+        f.x.copy_(hx, non_blocking=True)
 
-    def run_step(i):
-        k = i % 2
-        f, (h_init, h_resi, h_fin) = flows[k], hbufs[k]
-        f.s.wait_event(ev_in[k])
-        f.s.wait_event(ev_out[k])  # the previous step of this flow has been copied out
-        with torch.cuda.stream(f.s):
-            f.step()
-        ev_done[k].record(f.s)
-        cout.wait_event(ev_done[k])
-        with torch.cuda.stream(cout):
-            h_init.copy_(f.init[:s_init], non_blocking=True)
-            h_resi.copy_(f.resi[:s_resi], non_blocking=True)
-            h_fin.copy_(f.fin, non_blocking=True)
-        ev_out[k].record(cout)
+    def run(i, f, s):
+        f.step()
 
-    def e2e_run(n):
-        copy_in(0)
-        for i in range(n):
-            if i + 1 < n:
-                copy_in(i + 1)
-            run_step(i)
+    def store(i, f, s):
+        h_init, h_resi, h_fin = hbufs[i % 2]
+        h_init.copy_(f.init[:s_init], non_blocking=True)
+        h_resi.copy_(f.resi[:s_resi], non_blocking=True)
+        h_fin.copy_(f.fin, non_blocking=True)
 
+    pipe = Pipeline(dev, flows, load, run, store)
     e_steps = max(2, min(args.steps, 6))
-    e2e_run(2)
+    pipe(2)
+    pipe.sync()
     barrier(world)
     torch.cuda.synchronize(dev)
-    start.record(cin)
-    e2e_run(e_steps)
-    end.record(cout)
+    start.record(pipe.s_in)
+    pipe(e_steps)
+    end.record(pipe.s_out)
     torch.cuda.synchronize(dev)
     e2e_ok = bool(torch.equal(hbufs[0][2], fl.fin.cpu())) and bool(torch.equal(hbufs[1][2], hbufs[0][2]))
     e2e_ms = max_over_ranks(start.elapsed_time(end) / e_steps, world, dev)
