@@ -39,6 +39,7 @@ SIGNATURES = {
     "cortado_verify_bound": (_int, [_vp, _vp, _vp, _i64, _f32, _vp, _vp]),
     "cortado_set_launch_ctas": (_int, [_vp, _int, _int]),
     "cortado_reserve": (_int, [_vp, _i64, _int]),
+    "cortado_selftest_timeout": (_int, [_vp, _vp]),
 }
 
 OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5}

@@ -934,6 +934,14 @@ __global__ void k_range_publish(unsigned int* words, volatile unsigned int* host
   __threadfence_system();
 }
 
+// Failure-detection self-test: one thread waits, through the decoders' own
+// bounded wait, for a payload offset tagged with epoch 0x10000.  Lookback and
+// offset words carry a 16-bit epoch, so no launch can ever publish it; the
+// wait runs out after the context's timeout, latches DST_TIMEOUT and returns.
+__global__ void k_wait_selftest(Sync sy) {
+  if (threadIdx.x == 0) (void)wait_offset(sy, 0x10000u, 0);
+}
+
 }  // namespace
 
 // ================================================================== host side
@@ -1191,6 +1199,14 @@ cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas
     return CORTADO_ERR_INVALID_ARG;
   ctx->ctas_override[op] = ctas_per_sm;
   return CORTADO_OK;
+}
+
+cortado_status cortado_selftest_timeout(cortado_ctx* ctx, cortado_stream_t stream) {
+  if (!ctx) return CORTADO_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const Sync sy = next_sync(ctx, st);  // offs holds at least 1024 words from creation
+  k_wait_selftest<<<1, 32, 0, st>>>(sy);
+  return from_cuda(cudaGetLastError());
 }
 
 cortado_status cortado_sync(cortado_ctx* ctx, cortado_stream_t stream) {

@@ -86,6 +86,11 @@ class Codec:
     def set_timeout(self, seconds: float):
         check(self._L.cortado_set_timeout(self._h, int(seconds * 1e9)), "set_timeout")
 
+    def selftest_timeout(self, stream=None):
+        """Enqueues a bounded device wait that cannot succeed; the next sync()
+        raises CortadoError TIMEOUT once the context's timeout has passed."""
+        check(self._L.cortado_selftest_timeout(self._h, _stream(stream)), "selftest_timeout")
+
     def reserve(self, chunks: int, items: int = 0):
         """Sizes the scratch for calls of up to `chunks` chunks (all items of a
         batched call together) and `items` batch items, so that no later call

@@ -158,6 +158,14 @@ typedef struct {
 cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item* items, int n_items,
                              cortado_stream_t stream);
 
+/* Failure-detection self-test: launches one thread that waits, through the
+ * same bounded wait the decoders use for payload offsets, on a word that no
+ * launch can publish.  After the context's timeout (cortado_set_timeout) the
+ * wait gives up and latches CORTADO_ERR_TIMEOUT, which the next
+ * cortado_sync() returns (and clears); the context stays usable.  No
+ * counterpart in the reference (its waits are unbounded). */
+cortado_status cortado_selftest_timeout(cortado_ctx* ctx, cortado_stream_t stream);
+
 /* Sizes the context's scratch ahead of use: lookback and payload-offset words
  * for `chunks` chunks in one call (a batched call counts the chunks of all its
  * items), and batch item tables of `items` entries.  Calls that find their
