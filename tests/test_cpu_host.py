@@ -3,10 +3,8 @@ and of the C-ABI library's load and exports (no compute calls without a GPU)."""
 import ctypes
 import os
 import re
-import subprocess
 
 import numpy as np
-import pytest
 
 from cortado_b200 import storage
 

@@ -1,7 +1,6 @@
 """The batched form (cortado_batch): one launch over many streams of uneven
 sizes must produce exactly what one call per stream produces, for every
 operation, including partial last chunks and one-chunk fields."""
-import numpy as np
 import pytest
 import torch
 

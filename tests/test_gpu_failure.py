@@ -4,7 +4,6 @@ TIMEOUT status from sync(), the status is cleared, and the same context then
 encodes and decodes correctly."""
 import numpy as np
 import pytest
-import torch
 
 from cortado_b200 import fields
 from oracle import oracle as O
