@@ -657,6 +657,22 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
         const long long gp = __shfl_sync(0xffffffffu, pending, 0);
         if (lane == 0) pending = atomicAdd(&sy.counter[0], 1u);
         prefetch_stream(sm, s ^ 1, gp, src, ws);
+        if (OP == OP_RAPPLY && lane == 0) {
+          // When the next payload fills at most the first KiB of the other
+          // stage buffer, this chunk's client floats are loaded behind it
+          // (1024-byte aligned) now, overlapping the decode, instead of into
+          // this stage's buffer once the decode has read it back.  A next
+          // chunk that is present and usable means prefetch_stream has waited
+          // for that buffer's previous TMA store and fenced the proxies.
+          const StageMeta& mn = sm.st[s ^ 1];
+          const bool side = full && A.has_map_in && m.bad == 0 && mn.g < src.total && mn.bad == 0 &&
+                            mn.tma_len <= 1024 && mn.d + mn.csize <= 1024;
+          sm.src_side = side ? 1u : 0u;
+          if (side) {
+            mbar_expect_tx(&sm.bar_src, CS);
+            tma_load_rows(stage_buf(sm, s ^ 1) + 256, src.min(item), (int)(c * 128), &sm.bar_src);
+          }
+        }
       }
     };
     uint32_t v[32];
@@ -675,11 +691,15 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
     if (OP == OP_RAPPLY) {
       // d_iRESI_4 (d_RESI_4.h:79-94): requantize the client's floats to the
       // destination bound, add the residual, dequantize.  The client's chunk
-      // comes into the stage buffer once the decoder has read it back.
-      __syncthreads();
+      // is behind the next payload (sm.src_side) or comes into this stage's
+      // buffer once the decoder has read it back.
+      __syncthreads();  // sm.src_side
       const bool src_tma = full && A.has_map_in;
+      const uint32_t* S = P;  // where the client's chunk is
       if (src_tma) {
-        if (tid == TMA_TID) {
+        if (sm.src_side) {
+          S = stage_buf(sm, s ^ 1) + 256;
+        } else if (tid == TMA_TID) {
           fence_proxy_async();
           mbar_expect_tx(&sm.bar_src, CS);
           tma_load_rows(P, src.min(item), (int)(c * 128), &sm.bar_src);
@@ -691,7 +711,7 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
         __syncthreads();
       }
       uint32_t s2[32];
-      row_load(P, tid, s2);
+      row_load(S, tid, s2);
       // float forms when every word of the warp is lossy (client float, then
       // sum).  A per-word choice with the integer forms out of line, as in the
       // encoders, measured 12% slower here: both arrays then live in memory.

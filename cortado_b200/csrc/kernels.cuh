@@ -79,6 +79,7 @@ struct __align__(16) Ctl {
   Pend pend[2];             // encoders: the chunk of each stage, until it is flushed
   unsigned long long payload_off;
   unsigned int epoch, is_last;
+  unsigned int src_side;    // resi_recv: this chunk's client floats are behind the next payload
   uint32_t info[8];
 };
 static_assert(sizeof(Ctl) <= CTL_BYTES, "control block");
