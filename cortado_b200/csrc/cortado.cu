@@ -620,8 +620,10 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
 
 // storage decode / init_recv / resi_recv (d_server_decode_kernel,
 // d_client_decode_kernel, d_residual_apply_kernel).  The payload is expanded
-// in place in its stage buffer, which then takes resi_recv's client chunk and
-// stages the output floats for one TMA store.
+// in place in its stage buffer, which then stages the output floats for one
+// TMA store.  resi_recv's client chunk is loaded behind the next payload in
+// the other stage buffer when that payload is small, else into this stage's
+// buffer after the decode.
 template <int OP, class Src>
 __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;

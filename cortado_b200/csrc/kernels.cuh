@@ -33,7 +33,7 @@ struct OpArgs {
 };
 
 // ---------------------------------------------------------------- shared memory
-// A CTA owns a 1 KiB control block followed by 2 or 3 chunk buffers of
+// A CTA owns a 1 KiB control block followed by two chunk buffers of
 // BUF_WORDS words (16 KiB + slack, a multiple of 1024 bytes so that every
 // buffer keeps the 1024-byte alignment TMA's 128B swizzle needs).  How the
 // loops use them is described at each loop (cortado.cu).
