@@ -390,31 +390,28 @@ __device__ __forceinline__ void flush_pending(Ctl& sm, const Src& src, int t, co
   }
 }
 
-// The integer quantizer forms for the words (bit k of m) that the encoders'
-// fast forms cannot take.  The choice is per word, so one outlier no longer
-// sends its warp's 1024 words down the slow path.  Out of line: such words are
-// rare (lossless words, inf, NaN, raw chunks), and inlining the slow forms 32
-// times over made the loops large enough to stall on instruction fetch.
-__device__ __noinline__ void sq_words(uint32_t (&v)[32], uint32_t m, Quant q) {
-  for (; m; m &= m - 1) {
-    const int k = __ffs(m) - 1;
-    v[k] = sq_enc(v[k], q);
-  }
-}
 // Requantization through floats (d_s2c.h:132-137, d_RESI_4.h:57-76): the
 // stored bin (or, for a raw chunk, the float itself) -> float (iSQ) -> request
 // bin (CQ), or residual = destination bin minus the request bin requantized
-// to the destination bound.
+// to the destination bound.  For the words (bit k of m) that the shift form
+// cannot take; the choice is per word, so one outlier no longer sends its
+// warp's 1024 words down the slow path.  Out of line: such words are rare
+// (lossless words, raw chunks), and inlining the integer forms 32 times over
+// made the loop large enough to stall on instruction fetch.  The words are
+// the calling thread's own row of a swizzled buffer (row_store before the
+// call, row_load after): a pointer to the caller's register array would put
+// that array in local memory for the whole loop.
 template <int OP>
-__device__ __noinline__ void requant_words(uint32_t (&v)[32], uint32_t m, bool raw, Quant qs, Quant q1, Quant q2) {
+__device__ __noinline__ void requant_words(uint32_t* buf, uint32_t m, bool raw, Quant qs, Quant q1, Quant q2) {
+  const uint32_t base = 32u * threadIdx.x;
   for (; m; m &= m - 1) {
-    const int k = __ffs(m) - 1;
-    const uint32_t x = raw ? v[k] : iq_dec(v[k], qs);
+    const uint32_t w = swz(base + __ffs(m) - 1);
+    const uint32_t x = raw ? buf[w] : iq_dec(buf[w], qs);
     if (OP == OP_S2C) {
-      v[k] = cq_enc(x, q1);
+      buf[w] = cq_enc(x, q1);
     } else {
       const uint32_t src_req = cq_enc(iq_dec(cq_enc(x, q1), q1), q2);
-      v[k] = cq_enc(x, q2) - src_req;
+      buf[w] = cq_enc(x, q2) - src_req;
     }
   }
 }
@@ -468,17 +465,19 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
     row_load(A, tid, v);
     const Quant q1 = A_.q1;
     {
-      // the float form for words below the lossless threshold; the others
-      // (lossless words, inf, NaN) out of line
+      // the float form; a warp that holds lossless words (inf, NaN included)
+      // chooses per word
       const FastQ fq = make_fastq(q1.eb_e);
-      uint32_t slow = 0;
+      uint32_t amax = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) {
-        const bool ok = (v[k] & 0x7fffffffu) < fq.thr_bits;
-        slow |= (ok ? 0u : 1u) << k;
-        v[k] = ok ? sq_fast(v[k], fq) : v[k];
+      for (int k = 0; k < 32; k++) amax = max(amax, v[k] & 0x7fffffffu);
+      if (!__any_sync(0xffffffffu, amax >= fq.thr_bits)) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = sq_fast(v[k], fq);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = sq_mixed(v[k], fq, q1);
       }
-      if (slow) sq_words(v, slow, q1);
     }
     auto flush_prev = [&]() {
       flush_pending(sm, src, s ^ 1, B, raw_word);
@@ -488,7 +487,8 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
       encode_stage<true>(sm, A_.sy, v, A, B, c, nw, item, sm.pend[s], flush_prev);
     } else {
       flush_prev();
-      encode_stage_partial(sm, A_.sy, v, A, B, c, nw, item, sm.pend[s]);
+      row_store(A, tid, v);
+      encode_stage_partial(sm, A_.sy, A, B, c, nw, item, sm.pend[s]);
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
     __syncthreads();  // buffer 0 has been read
@@ -557,8 +557,12 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
     };
     uint32_t v[32];
     bool raw;
-    if (nw == CW) decode_core<true>(sm, A.sy, m, X, X, v, raw, NoHook{});
-    else decode_core_partial(sm, A.sy, m, X, X, v, raw, NoHook{});
+    if (nw == CW) {
+      decode_core<true>(sm, A.sy, m, X, X, v, raw, NoHook{});
+    } else {
+      raw = decode_core_partial(sm, A.sy, m, X, X, NoHook{});
+      row_load(X, tid, v);
+    }
     if (m.bad >= 2) {  // unusable stream header (batched): nothing to write
       if (tid == 0) sm.pend[s].valid = 0;
       flush_prev();
@@ -597,13 +601,18 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
         slow |= (ok ? 0u : 1u) << k;
         v[k] = ok ? (r ^ neg) - neg : v[k];
       }
-      if (slow) requant_words<OP>(v, slow, raw, qs, q1, q2);
+      if (slow) {  // after the decoder's last barrier row tid of X is this thread's own
+        row_store(X, tid, v);
+        requant_words<OP>(X, slow, raw, qs, q1, q2);
+        row_load(X, tid, v);
+      }
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
       if (nw == CW) {
         encode_stage<true>(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s], flush_prev);
       } else {
         flush_prev();
-        encode_stage_partial(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s]);
+        row_store(X, tid, v);
+        encode_stage_partial(sm, A.sy, X, Y, c, nw, item, sm.pend[s]);
         __syncthreads();  // sm.pend[s]
       }
       if (sm.pend[s].raw) {
@@ -683,7 +692,8 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
       decode_core<true>(sm, A.sy, m, P, P, v, raw, next);
     } else {
       next();
-      decode_core_partial(sm, A.sy, m, P, P, v, raw, NoHook{});
+      raw = decode_core_partial(sm, A.sy, m, P, P, NoHook{});
+      row_load(P, tid, v);
     }
     if (m.bad >= 2) {  // unusable stream header (batched): nothing to write
       __syncthreads();
@@ -712,43 +722,70 @@ __device__ __forceinline__ void decode_loop(Ctl& sm, const Src& src, const Sync&
         load_plain_rows(P, A.src, c, nw);
         __syncthreads();
       }
-      uint32_t s2[32];
-      row_load(S, tid, s2);
-      // float forms when every word of the warp is lossy (client float, then
-      // sum).  A per-word choice with the integer forms out of line, as in the
-      // encoders, measured 12% slower here: both arrays then live in memory.
+      // The client's words are read from shared memory 16 bytes at a time
+      // and folded into v in place (client bin + residual), so only one
+      // 32-word array is live.  The float forms, chosen per word in a warp
+      // that holds lossless client words or bins.
+      const uint4* Srow = reinterpret_cast<const uint4*>(S + 32 * tid);
       const FastQ fq = make_fastq(m.eb_e);
       uint32_t amax = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) amax = max(amax, s2[k] & 0x7fffffffu);
-      if (__all_sync(0xffffffffu, amax < fq.thr_bits)) {
+      for (int u = 0; u < 8; u++) {
+        const uint4 w = Srow[u ^ (tid & 7)];
+        amax = max(amax, max(max(w.x & 0x7fffffffu, w.y & 0x7fffffffu), max(w.z & 0x7fffffffu, w.w & 0x7fffffffu)));
+      }
+      if (!__any_sync(0xffffffffu, amax >= fq.thr_bits)) {
 #pragma unroll
-        for (int k = 0; k < 32; k++) s2[k] = cq_fast(s2[k], fq) + v[k];
+        for (int u = 0; u < 8; u++) {
+          const uint4 w = Srow[u ^ (tid & 7)];
+          v[4 * u] += cq_fast(w.x, fq);
+          v[4 * u + 1] += cq_fast(w.y, fq);
+          v[4 * u + 2] += cq_fast(w.z, fq);
+          v[4 * u + 3] += cq_fast(w.w, fq);
+        }
       } else {
 #pragma unroll
-        for (int k = 0; k < 32; k++) s2[k] = cq_enc(s2[k], q) + v[k];
+        for (int u = 0; u < 8; u++) {
+          const uint4 w = Srow[u ^ (tid & 7)];
+          v[4 * u] += cq_mixed(w.x, fq, q);
+          v[4 * u + 1] += cq_mixed(w.y, fq, q);
+          v[4 * u + 2] += cq_mixed(w.z, fq, q);
+          v[4 * u + 3] += cq_mixed(w.w, fq, q);
+        }
       }
       uint32_t bmax = 0;
 #pragma unroll
       for (int k = 0; k < 32; k++) {
-        const uint32_t neg = (uint32_t)((int32_t)s2[k] >> 31);
-        bmax = max(bmax, (s2[k] ^ neg) - neg);
+        const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
+        bmax = max(bmax, (v[k] ^ neg) - neg);
       }
       if (__all_sync(0xffffffffu, bmax < 0x800000u)) {
 #pragma unroll
-        for (int k = 0; k < 32; k++) v[k] = iq_fast(s2[k], fq);
+        for (int k = 0; k < 32; k++) v[k] = iq_fast(v[k], fq);
       } else {
 #pragma unroll
-        for (int k = 0; k < 32; k++) v[k] = iq_dec(s2[k], q);
+        for (int k = 0; k < 32; k++) v[k] = iq_mixed(v[k], fq, q);
       }
     } else if (!raw) {
       // chunks stored uncompressed are copied out as stored: original floats
       // for storage decode (d_server_encode.h:234-249), request bins for
       // init_recv (d_client_encode.h:230-254, the reference's behaviour).
-      // (The float dequantizer, chosen per warp as in resi_recv, measured no
-      // faster here and 4% slower on dense data.)
+      // The float dequantizer, chosen per word in a warp that holds lossless
+      // bins.
+      const FastQ fq = make_fastq(m.eb_e);
+      uint32_t bmax = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = iq_dec(v[k], q);
+      for (int k = 0; k < 32; k++) {
+        const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
+        bmax = max(bmax, (v[k] ^ neg) - neg);
+      }
+      if (__all_sync(0xffffffffu, bmax < 0x800000u)) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = iq_fast(v[k], fq);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = iq_mixed(v[k], fq, q);
+      }
     }
     row_store(P, tid, v);  // every plane read finished before the decoder's last barrier
     const bool tma_out = full && A.has_map_out;

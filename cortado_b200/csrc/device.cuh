@@ -222,6 +222,28 @@ __device__ __forceinline__ uint32_t iq_fast(uint32_t enc, const FastQ& f) {
   return __float_as_uint(__fmul_rn(__int2float_rn((int)enc), f.dsc));
 }
 
+// Per-word forms for warps that hold lossless words.  A lossless word (|x| at
+// or above the threshold, inf and NaN included) has SQ and CQ bin
+// +-(|x| - offs) (the exponent branch of d_SQ_IABS_4.h:62-76 and
+// d_CQ_IABS_4.h:62-77), and a bin of magnitude 2^23 or more dequantizes to
+// |b| + offs with b's sign bit (d_SQ_IABS_4.h:90-107); every other word takes
+// the float form.  Inline selects, so no call keeps a register array live.
+__device__ __forceinline__ uint32_t lossless_bin(uint32_t v, const Quant& q) {
+  const uint32_t s = (uint32_t)((int32_t)v >> 31);
+  return (((v & 0x7fffffffu) - (uint32_t)q.offs) ^ s) - s;
+}
+__device__ __forceinline__ uint32_t sq_mixed(uint32_t v, const FastQ& f, const Quant& q) {
+  return (v & 0x7fffffffu) < f.thr_bits ? sq_fast(v, f) : lossless_bin(v, q);
+}
+__device__ __forceinline__ uint32_t cq_mixed(uint32_t v, const FastQ& f, const Quant& q) {
+  return (v & 0x7fffffffu) < f.thr_bits ? cq_fast(v, f) : lossless_bin(v, q);
+}
+__device__ __forceinline__ uint32_t iq_mixed(uint32_t b, const FastQ& f, const Quant& q) {
+  const uint32_t neg = (uint32_t)((int32_t)b >> 31);
+  const uint32_t a = (b ^ neg) - neg;
+  return a < 0x800000u ? iq_fast(b, f) : ((a + (uint32_t)q.offs) | (b & 0x80000000u));
+}
+
 // ---------------------------------------------------------------- BIT_4
 // The reference's BIT_4 warp butterfly (include/components/d_BIT_4.h:41-92)
 // maps input word i, bit b of a 32-word group to output plane 31-b, bit 31-i:

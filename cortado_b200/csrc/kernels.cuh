@@ -671,22 +671,31 @@ __device__ __forceinline__ void decode_core(Ctl& sm, const Sync& sy, const Stage
 
 // The partial last chunk of a stream (at most one per stream) runs out of
 // line, so the full-chunk loop body stays small enough for the instruction
-// caches.  Arrays pass through local memory on this rare path.
-__device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint32_t* v, uint32_t* plane, uint8_t* st,
-                                                  long long c, int nw, int item, Pend& pend) {
+// caches.  Its words pass through the calling thread's own row of the plane
+// buffer (row tid = linear words 32*tid .. 32*tid+31), never through a pointer
+// to the caller's register array: taking that array's address would put it in
+// local memory on the hot full-chunk path as well.
+// encode_stage_partial: the caller has stored its group's words in row tid of
+// `plane` (row_store).
+__device__ __noinline__ void encode_stage_partial(Ctl& sm, const Sync& sy, uint32_t* plane, uint8_t* st, long long c,
+                                                  int nw, int item, Pend& pend) {
   uint32_t w[32];
-#pragma unroll
-  for (int k = 0; k < 32; k++) w[k] = v[k];
+  row_load(plane, threadIdx.x, w);
   encode_stage<false>(sm, sy, w, plane, st, c, nw, item, pend, NoHook{});
 }
 
+// decode_core_partial: leaves the group's words in row tid of `plane` (the
+// caller reads them back with row_load) and returns whether the chunk was
+// stored uncompressed.  decode_core ends with a barrier after which no thread
+// reads another thread's row, so each thread may overwrite its own.
 template <typename Side>
-__device__ __noinline__ void decode_core_partial(Ctl& sm, const Sync& sy, const StageMeta& m, uint32_t* P,
-                                                 uint32_t* plane, uint32_t* v, bool& raw_out, Side side) {
+__device__ __noinline__ bool decode_core_partial(Ctl& sm, const Sync& sy, const StageMeta& m, uint32_t* P,
+                                                 uint32_t* plane, Side side) {
   uint32_t w[32];
-  decode_core<false>(sm, sy, m, P, plane, w, raw_out, side);
-#pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = w[k];
+  bool raw = false;
+  decode_core<false>(sm, sy, m, P, plane, w, raw, side);
+  row_store(plane, threadIdx.x, w);
+  return raw;
 }
 
 }  // namespace cortado
