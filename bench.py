@@ -19,7 +19,9 @@ the field from pinned host memory to the device and copies the two streams
 sent to the client and the final reconstruction back.
 
 --impl reference times the reference path's CPU counterpart (the C oracle,
-OpenMP over chunks, all host threads) on a bounded sample of the same field.
+OpenMP over chunks, all host threads) on the same whole field.  ``ref_cuda``
+holds the reference's own CUDA build timed on the same field, bounds and GPU
+(its benchmark binaries, inside the clock-sampled window).
 """
 from __future__ import annotations
 
@@ -308,8 +310,14 @@ def _run_gpu(args, rank, world):
     abs_ms = max_over_ranks(start.elapsed_time(end) / a_steps, world, dev)
     codec.sync(stream)
     abs_res = dict(ms=abs_ms, per_op=a_op / a_steps, sizes=abs_sizes, ok=abs_ok)
+    x_host = x.cpu().numpy()
+    # The reference's own CUDA build on the same field, bounds and GPU, in the
+    # same clock-sampled window (a reported baseline; one GPU only).
+    ref_cuda = None
+    if world == 1 and not args.no_ref_cuda:
+        ref_cuda = reference_cuda_baseline(x_host)
     return dict(abs=abs_res, ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
-                h2d=n, d2h=s_init + s_resi + n)
+                h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda)
 
 
 def barrier(world):
@@ -338,12 +346,8 @@ def bench_batched(codec, dev, n_fields=64, seed=3, max_mb=256, bounds=("1e-1", "
     NOA bounds -- one batched launch vs one launch per (field, bound)."""
     from cortado_b200 import fields, storage
     from cortado_b200.ops import max_stream_bytes
-    rng = np.random.Generator(np.random.PCG64(seed))
-    kinds = ("sinusoid", "grf", "white")
-    xs = []
-    for i in range(n_fields):
-        nb = int(np.exp(rng.uniform(np.log(1 << 20), np.log(max_mb << 20)))) & ~3
-        xs.append(fields.mixed_field(nb // 4, kinds[i % 3], seed * 1000 + i, device=dev))
+    xs = [fields.mixed_field(nf, kind, fs, device=dev)
+          for nf, kind, fs in fields.field_set(n_fields, seed, 1 << 20, max_mb << 20)]
     items, outs = [], []
     sizes = torch.zeros(len(xs) * len(bounds), dtype=torch.int64, device=dev)
     for i, x in enumerate(xs):
@@ -395,11 +399,9 @@ def bench_serving(dev, n_fields=32, n_requests=400, rates=(2000.0, 8000.0, 32000
     from cortado_b200.serve import Server, poisson_trace
     rng = np.random.Generator(np.random.PCG64(seed))
     srv = Server(dev.index, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3, max_batch=16)
-    kinds = ("sinusoid", "grf", "white")
     ranges = {}
-    for i in range(n_fields):
-        nb = int(np.exp(rng.uniform(np.log(4 << 20), np.log(max_mb << 20)))) & ~3
-        x = fields.mixed_field(nb // 4, kinds[i % 3], seed * 1000 + i, device=dev)
+    for i, (nf, kind, fs) in enumerate(fields.field_set(n_fields, seed, 4 << 20, max_mb << 20, rng=rng)):
+        x = fields.mixed_field(nf, kind, fs, device=dev)
         r = float(x.max() - x.min())
         ranges[f"f{i}"] = r
         srv.add_field(f"f{i}", x, [float(storage.noa_scale(e, r)) for e in (1e-1, 1e-3, 1e-5, 1e-7)])
@@ -495,13 +497,23 @@ def load_traffic():
     return {}
 
 
-def cpu_baseline(sample_mb=64, threads=None):
-    """The C oracle on a sample of the field: the same six operations."""
-    from cortado_b200 import fields, storage
+def host_field(shape, seed=2, sample_mb=0) -> np.ndarray:
+    """The benchmark field's bytes in host memory, generated on the GPU when
+    one is present (the same bytes the GPU arm times), else on the CPU.
+    sample_mb > 0 builds a smaller field of about that many MiB instead (the
+    same generator on fewer z-planes; CPU tests only)."""
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    if sample_mb > 0:
+        shape = (max(1, sample_mb * (1 << 20) // (4 * shape[1] * shape[2])), shape[1], shape[2])
+    return make_field(seed, dev, shape).cpu().numpy()
+
+
+def cpu_step(x: np.ndarray, threads: int) -> float:
+    """One step of the benchmark flow (NOA range, store, init_send, init_recv,
+    resi_send, resi_recv) through the CPU oracle on `threads` host threads;
+    returns its duration in seconds."""
+    from cortado_b200 import storage
     from oracle import oracle as O
-    nw = sample_mb * (1 << 20) // 4
-    x = fields.sinusoid((nw // (512 * 512), 512, 512), 2, outlier_frac=1e-3).reshape(-1).numpy()
-    threads = threads or os.cpu_count()
     t0 = time.perf_counter()
     rng = O.noa_range(x)
     eb_s, eb_a, eb_b = (float(storage.noa_scale(e, rng)) for e in (EB_STORE, EB_SRC, EB_DST))
@@ -510,9 +522,71 @@ def cpu_baseline(sample_mb=64, threads=None):
     cl = O.init_recv(init, threads)
     resi = O.resi_send(stor, eb_a, eb_b, threads)
     O.resi_recv(cl, resi, threads)
-    dt = time.perf_counter() - t0
-    return {"value": x.nbytes * 1e-9 / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample_mb} MiB slice (first {nw // (512 * 512)} of 512 z-planes) of the field, one step of the six operations"}
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(x: np.ndarray, steps=1, warmup=1, threads=None):
+    """The C oracle (OpenMP over chunks, all host threads) on the whole
+    benchmark field: `warmup` untimed steps, then `steps` timed ones."""
+    threads = threads or os.cpu_count()
+    for _ in range(warmup):
+        cpu_step(x, threads)
+    total = sum(cpu_step(x, threads) for _ in range(steps))
+    ms = total * 1e3 / steps
+    return {"value": x.nbytes * 1e-9 / (ms * 1e-3), "unit": UNIT, "cores": threads, "kind": "port",
+            "ms_per_step": ms, "steps": steps,
+            "sample": f"the whole field ({x.nbytes} bytes), every operation of the step, {steps} timed step(s) "
+                      f"after {warmup} warm-up"}
+
+
+def reference_cuda_baseline(x: np.ndarray, timeout_s=120):
+    """The reference's own CUDA build (its benchmark binaries, compiled from its
+    sources for sm_100a into oracle/_ref) on the same field and bounds, NOA
+    and ABS: each operation's median of 10 runs as those binaries report it
+    (host-side timer around the wrapper, which allocates and frees its carry
+    array per call; src/cortado_store.cu:239-245, src/cortado_init.cu:448,549,
+    src/cortado_resi.cu:509,641).  A reported baseline, never the measured
+    product."""
+    import re
+    import shutil
+    import tempfile
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    bins = {b: os.path.join(ref, b) for b in ("store_bench", "init_bench", "resi_bench")}
+    if not all(os.access(p, os.X_OK) for p in bins.values()):
+        return {"unavailable": "oracle/_ref benchmark binaries not built (the reference sources were absent at build)"}
+    d = tempfile.mkdtemp(prefix="cortado_refcuda_")
+    f = os.path.join(d, "field.f32")
+    x.tofile(f)
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+        if r.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(cmd[0])} rc={r.returncode}: {r.stderr[-300:]}")
+        return r.stdout
+
+    def msecs(out, key):
+        m = re.findall(rf"^{key}:\s+([0-9.]+) s", out, re.M)
+        return float(m[-1]) * 1e3 if m else None
+
+    res = {"kind": "reference CUDA build", "runs": 10,
+           "timer": "the reference binaries' own: median of 10 runs after a warm-up, wrapper-inclusive"}
+    try:
+        for mode, (st, a, b), flag in (("noa", (EB_STORE, EB_SRC, EB_DST), []),
+                                       ("abs", (ABS_STORE, ABS_SRC, ABS_DST), ["-a"])):
+            o1 = run([bins["store_bench"], f, st, "-r", "10", *flag])
+            o2 = run([bins["init_bench"], f, st, a, "-r", "10", *flag])
+            o3 = run([bins["resi_bench"], f, st, a, b, "-r", "10", *flag])
+            ops = {"store": msecs(o1, "runtime"), "init_send": msecs(o2, "send runtime"),
+                   "init_recv": msecs(o2, "recv runtime"), "resi_send": msecs(o3, "send runtime"),
+                   "resi_recv": msecs(o3, "recv runtime")}
+            if any(v is None for v in ops.values()):
+                raise RuntimeError(f"no runtime line in the {mode} output")
+            res[mode] = {"ms": ops, "sum_ms": sum(ops.values())}
+    except (RuntimeError, subprocess.TimeoutExpired, OSError) as e:
+        res = {"unavailable": f"reference binaries failed: {e}"}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return res
 
 
 def main():
@@ -521,7 +595,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cortado_b200", choices=["cortado_b200", "reference"])
-    ap.add_argument("--cpu-sample-mb", type=int, default=64)
+    ap.add_argument("--cpu-sample-mb", type=int, default=0,
+                    help="CPU legs on a smaller field of about this many MiB (0: the whole field)")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA build")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="512,512,512", help="field shape (profiling uses a smaller one)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
@@ -538,16 +614,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        x = host_field(args.shape, 2, args.cpu_sample_mb)
         k = max(1, args.steps)
-        vals = []
-        for _ in range(min(args.warmup, 1)):
-            cpu_baseline(args.cpu_sample_mb)
-        for _ in range(k):
-            vals.append(cpu_baseline(args.cpu_sample_mb))
-        v = float(np.median([b["value"] for b in vals]))
-        base = dict(vals[0], value=v)
+        base = cpu_baseline(x, steps=k, warmup=args.warmup)
+        v = base["value"]
+        cfg["field_bytes"] = int(x.nbytes)
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-                          "steps": k, "warmup": args.warmup, "ms_per_step": cfg["field_bytes"] * 1e-6 / v,
+                          "steps": k, "warmup": args.warmup, "ms_per_step": base["ms_per_step"],
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32",
                           "data": "synthetic", "config": cfg, "cpu_baseline": base,
                           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
@@ -599,6 +672,15 @@ def main():
                              for k, t in zip(OPS, r["abs"]["per_op"])}},
         "clocks": r["clocks"],
     }
+    if r["ref_cuda"] is not None:
+        rc = r["ref_cuda"]
+        if "noa" in rc:  # set beside this run's own per-operation times
+            mine_abs = {k: t for k, t in zip(OPS, r["abs"]["per_op"]) if k in alg}
+            rc["cortado_b200_ms"] = {"noa": {k: op_ms[k] for k in alg}, "abs": mine_abs,
+                                     "noa_reference_style": {k: r["ref_style"][k] for k in alg}}
+            rc["speedup_sum_of_ops"] = {"noa": rc["noa"]["sum_ms"] / sum(op_ms[k] for k in alg),
+                                        "abs": rc["abs"]["sum_ms"] / sum(mine_abs.values())}
+        line["ref_cuda"] = rc
     if not args.no_extras and world == 1:
         from cortado_b200.ops import Codec
         dev = torch.device("cuda", 0)
@@ -613,7 +695,7 @@ def main():
         c.close()
         torch.cuda.empty_cache()
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_sample_mb)
+        line["cpu_baseline"] = cpu_baseline(r["x_host"])
     print(json.dumps(line))
 
 

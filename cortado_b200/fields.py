@@ -108,3 +108,20 @@ def mixed_field(n_floats: int, kind: str, seed: int, device="cpu") -> torch.Tens
     else:
         raise ValueError(kind)
     return f.reshape(-1)[:n_floats].contiguous()
+
+
+def field_set(n_fields: int, seed: int, min_bytes: int, max_bytes: int, rng=None):
+    """Sizes, generators and seeds of a many-fields configuration: n_fields
+    sizes log-uniform in [min_bytes, max_bytes] (rounded down to a multiple of
+    4 bytes, so last chunks are partial), generators cycling sinusoid, GRF
+    (k^-3), white noise.  Returns [(n_floats, kind, field_seed)]; build a field
+    with mixed_field(*entry).  The sizes are drawn from `rng` when given (the
+    caller keeps drawing from it), else from a fresh PCG64(seed)."""
+    if rng is None:
+        rng = np.random.Generator(np.random.PCG64(seed))
+    kinds = ("sinusoid", "grf", "white")
+    out = []
+    for i in range(n_fields):
+        nb = int(np.exp(rng.uniform(np.log(min_bytes), np.log(max_bytes)))) & ~3
+        out.append((nb // 4, kinds[i % 3], seed * 1000 + i))
+    return out

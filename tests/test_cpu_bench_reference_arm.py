@@ -1,7 +1,8 @@
 """The benchmark's reference arm (bench.py --impl reference) runs on host cores
 only: one JSON line with the contract's keys, impl "reference", a
 cpu_baseline describing the run and an e2e entry with no host<->device bytes.
-A small sample keeps it to a few seconds here."""
+A small field keeps it to a few seconds here (the default is the whole
+512^3 field)."""
 import json
 import os
 import subprocess
@@ -28,3 +29,6 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["e2e"]["value"] == d["value"]
+    # ms_per_step is measured (the timed steps' mean), and value follows from it
+    assert abs(d["config"]["field_bytes"] * 1e-6 / d["ms_per_step"] - d["value"]) < 1e-9 * d["value"] + 1e-12
+    assert cb["ms_per_step"] == d["ms_per_step"] and cb["steps"] == d["steps"]
