@@ -11,8 +11,10 @@
  * Host-only logic: argument parsing, bound scaling (float arithmetic, as the
  * reference compiles with -ffp-contract=off), .stor.meta, stored-file choice.
  */
+#define _XOPEN_SOURCE 700 /* nftw */
 #include <cuda_runtime.h>
 #include <errno.h>
+#include <ftw.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -23,6 +25,34 @@
 
 #define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fprintf(stderr, "CUDA error %d on line %d: %s\n\n", (int)e_, __LINE__, cudaGetErrorString(e_)); exit(1); } } while (0)
 #define CS_(x, what) do { cortado_status s_ = (x); if (s_ != CORTADO_OK) { fprintf(stderr, "ERROR: %s: %s\n", what, cortado_status_string(s_)); exit(1); } } while (0)
+
+static int remove_entry(const char* path, const struct stat* sb, int flag, struct FTW* ftw) {
+  (void)sb;
+  (void)flag;
+  (void)ftw;
+  return remove(path); /* files, links, and directories once emptied (depth first) */
+}
+
+/* Deletes `dir` with everything in it, then creates it again with any missing
+ * parents: the reference's std::filesystem::remove_all + create_directories
+ * (src/cortado_store.cu:170-179), without a shell, so no character of the path
+ * is interpreted. */
+static int reset_dir(const char* dir) {
+  struct stat st;
+  if (lstat(dir, &st) == 0 && nftw(dir, remove_entry, 64, FTW_DEPTH | FTW_PHYS) != 0) return -1;
+  char buf[4096];
+  const size_t n = strlen(dir);
+  if (n == 0 || n >= sizeof buf) return -1;
+  memcpy(buf, dir, n + 1);
+  for (char* p = buf + 1; *p; p++) {
+    if (*p != '/') continue;
+    *p = 0;
+    if (mkdir(buf, 0777) != 0 && errno != EEXIST) return -1;
+    *p = '/';
+  }
+  if (mkdir(buf, 0777) != 0 && errno != EEXIST) return -1;
+  return 0;
+}
 
 static unsigned char* read_file(const char* name, long long* size) {
   FILE* f = fopen(name, "rb");
@@ -147,10 +177,9 @@ int main(int argc, char** argv) {
   neb = k;
   printf("%s error bounds (%d):\n", a.abs_mode ? "ABS" : "NOA", neb);
   for (int i = 0; i < neb; i++) printf("  %lf\n", ebs[i]);
-  if (a.o_dir) {
-    char cmd[4200];
-    snprintf(cmd, sizeof cmd, "rm -rf '%s' && mkdir -p '%s'", a.o_dir, a.o_dir);
-    if (system(cmd) != 0) { fprintf(stderr, "FILESYSTEM ERROR: %s\n", a.o_dir); return 1; }
+  if (a.o_dir && reset_dir(a.o_dir) != 0) {
+    fprintf(stderr, "FILESYSTEM ERROR: %s\n", a.o_dir);
+    return 1;
   }
   long long insize;
   unsigned char* h_in = read_file(input, &insize);

@@ -1,10 +1,13 @@
 # Builds the reference's eight CLI binaries from its own sources, in place under
-# REF (read-only), into oracle/_ref/.  Flags follow the reference Makefile
+# REF (read-only; required: make -f oracle/ref.mk REF=<reference checkout>),
+# into oracle/_ref/.  Flags follow the reference Makefile
 # (Makefile:1-4 there) with the device architecture fixed to sm_100a and a
 # portable host -march (the GPU box CPU may differ from the build host).  The binaries are
 # test infrastructure: they produce golden streams on a GPU box and are never
 # linked into or called by the product library.
-REF ?= /root/reference
+ifndef REF
+$(error REF=<path of the reference checkout> is required)
+endif
 OUT ?= $(dir $(lastword $(MAKEFILE_LIST)))_ref
 NVCC ?= nvcc
 FLAGS = -arch=sm_100a -O3 -DUSE_GPU -DNDEBUG -fmad=false \

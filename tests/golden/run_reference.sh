@@ -1,8 +1,8 @@
 #!/usr/bin/env bash
 # Runs the reference's own CLI binaries (built from its sources into
 # oracle/_ref by oracle/ref.mk) over every case in tests/golden/cases.json and
-# writes their streams, decoded files and logs under $1 (default
-# gpurun_out/golden).  Needs a GPU.  tests/golden/collect.py then turns the
+# writes their streams, decoded files and logs under $1 (default: a new
+# temporary directory, printed at the end).  Needs a GPU.  tests/golden/collect.py then turns the
 # outputs into tests/golden/reference_outputs.json (hashes + sizes).
 #
 # Usage: tests/golden/run_reference.sh [outdir] [extra_input.f32 ...]
@@ -10,7 +10,7 @@ set -u
 HERE="$(cd "$(dirname "$0")" && pwd)"
 ROOT="$(cd "$HERE/../.." && pwd)"
 REF="$ROOT/oracle/_ref"
-OUT="${1:-$ROOT/gpurun_out/golden}"
+OUT="${1:-$(mktemp -d "${TMPDIR:-/tmp}/cortado_golden.XXXXXX")}"
 shift || true
 mkdir -p "$OUT"
 python3 - "$HERE/cases.json" "$@" > "$OUT/plan.txt" << 'PY'

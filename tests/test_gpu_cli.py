@@ -59,3 +59,23 @@ def test_cli_files_match_reference(cuda_device, tmp_path, name, setting):
     if ref.get("resi_recv_deterministic", True):
         b = (tmp_path / "resi_dec.f32").read_bytes()
         assert {"sha256": hashlib.sha256(b).hexdigest(), "bytes": len(b)} == ref["resi_dec.f32"]
+
+
+def test_store_replaces_output_dir_without_a_shell(cuda_device, tmp_path):
+    """store -o deletes the output directory (with old contents, nested
+    directories included) and creates it again, as the reference's
+    std::filesystem calls do; no character of the path is interpreted (a
+    quote, a space, a semicolon and a $ stay part of the name)."""
+    build.build()
+    src = os.path.join(G.GOLDEN, "inputs", "sin3d_32.f32")
+    inp = tmp_path / "in.f32"
+    inp.write_bytes(open(src, "rb").read())
+    odd = "out dir 'q'; touch pwned; $HOME"
+    d = tmp_path / "a" / odd
+    (d / "old" / "deeper").mkdir(parents=True)
+    (d / "old" / "deeper" / "stale.bin").write_bytes(b"x")
+    (d / "stale.stor.07").write_bytes(b"y")
+    rc, out = _run([os.path.join(BIN, "store"), str(inp), "1e-2", "1e-4", "-o", str(d)], tmp_path)
+    assert rc == 0, out
+    assert sorted(os.listdir(d)) == [".stor.meta", "in.f32.stor.00", "in.f32.stor.01"]
+    assert not (tmp_path / "pwned").exists()
