@@ -1532,12 +1532,33 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
 }
 
 // Per-device set-up of the no-allocation entry point: the device address of
-// g_noalloc_scratch and the persistent grid size.
+// g_noalloc_scratch and the persistent grid size, valid for the CUDA context
+// that was current when they were looked up (a device reset or a new primary
+// context gets a new address, so a change of context repeats the set-up).
 struct NoallocDev {
   bool ready = false;
+  CUcontext ctx = nullptr;
   unsigned long long* scratch = nullptr;
   int grid = 0;
 };
+
+// The calling thread's current CUDA context (driver entry point, as for the
+// tensor-map encoder), or null when it cannot be queried.
+static CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Fn>(p);
+  });
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 static NoallocDev g_noalloc_dev[64];
 static std::mutex g_noalloc_mu;
 
@@ -1556,9 +1577,10 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
   if (dev < 0 || dev >= 64) return CORTADO_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   NoallocDev& d = g_noalloc_dev[dev];
+  const CUcontext cur = current_context();
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!d.ready) {
+    if (!d.ready || d.ctx != cur) {
       // device `dev` is current here
       void* p = nullptr;
       ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -1567,6 +1589,7 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       d.grid = occupancy_grid(k_store_noalloc, SMEM_STD, sms);
       d.scratch = (unsigned long long*)p;
+      d.ctx = cur;
       d.ready = true;
     }
   }

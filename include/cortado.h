@@ -202,6 +202,9 @@ cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas
  *     any stream capture;
  *   - all calls share the one array, so calls that overlap on the GPU (other
  *     streams, other host threads) race and give wrong output: serialize them;
+ *   - the set-up is repeated when the calling thread's CUDA context changes
+ *     (for example after cudaDeviceReset);
+ *   - every device-side wait gives up after a fixed 2 s;
  *   - there is no context to latch device-side errors in: a failed launch
  *     writes a negative status (-CORTADO_ERR_TIMEOUT) to *d_outsize. */
 #define CORTADO_NOALLOC_MAX_BYTES (1LL << 30)

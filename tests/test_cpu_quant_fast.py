@@ -1,8 +1,10 @@
 """The float forms of the quantizers that the kernels use for lossy words
 (server quantizer, client quantizer, dequantizer: a power-of-two scale and a
 truncating conversion) equal the oracle's integer restatements of the
-reference's d_SQ_IABS_4 / d_CQ_IABS_4 / d_iSQ_IABS_4 on every lossy input:
-all 2^32 words for two exponents and a stride-97 sweep for the extremes."""
+reference's d_SQ_IABS_4 / d_CQ_IABS_4 / d_iSQ_IABS_4 on every lossy input,
+and with the lossless shortcuts (+-(|x| - offs) and |b| + offs) on every
+other input: all 2^32 words for two exponents and a stride-97 sweep for the
+extremes."""
 import os
 import subprocess
 
