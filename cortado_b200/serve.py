@@ -25,11 +25,29 @@ with CUDA events.  A request's
 latency is its completion time (the host clock when its batch's event is seen
 complete) minus its arrival.
 
+Device memory is admitted against ``mem_cap_bytes``: resident stored streams,
+resident client reconstructions and output stream buffers (in flight or
+pooled for reuse) are counted.  A request's admission reserves its output
+buffer, its client's reconstruction (when that client has none resident)
+and its field's stored streams (when they are not resident).  When a request
+does not fit, idle state is spilled to host files until it does, least
+recently used first: pooled output buffers are freed, then idle clients'
+reconstructions are written as raw float32 files (the reference's
+decoded-file format, which its resi_recv reads back as the client's source,
+src/cortado_resi.cu:393-410), then idle fields' stored streams as a server
+storage directory (``<field>.stor.NN`` + ``.stor.meta``,
+include/util.h:70-135).  "Idle" means that no admitted, unfinished request
+uses it.  Spilled state is read back when a request needs it.  Only a
+request larger than the cap by itself is an error.
+
 ``run_plain`` serves the same trace with the plain per-request pipeline (one
 operation per launch, synchronized after each request) for comparison.
 """
 from __future__ import annotations
 
+import contextlib
+import os
+import tempfile
 import time
 from dataclasses import dataclass, field
 
@@ -57,16 +75,24 @@ class Field:
     name: str
     x: torch.Tensor                 # original floats (device), kept for verification only
     store_bounds: list              # absolute, descending
-    stored: list = field(default_factory=list)
+    stored: list = field(default_factory=list)        # device streams (empty while spilled)
     stored_bytes: list = field(default_factory=list)
+    vrange: float = 0.0             # max - min of the original (written to .stor.meta)
+    spilled: str | None = None      # storage directory holding the streams while not resident
+    last_use: int = 0
 
     @property
     def n_bytes(self):
         return self.x.numel() * 4
 
+    @property
+    def stored_total(self):
+        return sum(self.stored_bytes)
+
 
 class Server:
-    def __init__(self, device=0, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3, max_batch=16):
+    def __init__(self, device=0, mem_cap_bytes=120 * 10**9, max_inflight=64, n_streams=3, max_batch=16,
+                 spill_dir: str | None = None):
         self.dev = torch.device("cuda", device)
         self.codecs = [Codec(device) for _ in range(n_streams)]
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(n_streams)]
@@ -74,18 +100,26 @@ class Server:
         self.max_inflight = max_inflight
         self.max_batch = max_batch
         self.fields: dict[str, Field] = {}
-        self.clients: dict[tuple, dict] = {}   # (client, field) -> {"recon": tensor, "bound": float}
+        # (client, field) -> {"recon": tensor or None (not resident), "bound": float or None,
+        #                     "spilled": host file or None, "last_use": int}
+        self.clients: dict[tuple, dict] = {}
         self.mem_used = 0
+        self.spill_dir = spill_dir
+        self.spills = 0
+        self.reloads = 0
+        self._tick = 0
         # Output stream buffers, per field (each field's capacity is fixed),
         # reused once the batch that held one is seen complete: after a
         # warm-up the loop allocates no device memory.  (Allocating per request
         # through the caching allocator, across several streams, sometimes
-        # fell back to a fresh cudaMalloc, which stalls the device.)
+        # fell back to a fresh cudaMalloc, which stalls the device.)  Pooled
+        # buffers count against the memory cap until they are freed.
         self._free_out: dict[str, list[torch.Tensor]] = {}
 
     # ---------------------------------------------------------------- storage
-    def add_field(self, name, x, store_bounds_abs):
+    def add_field(self, name, x, store_bounds_abs, vrange=None):
         f = Field(name, x.contiguous().view(-1), sorted((float(e) for e in store_bounds_abs), reverse=True))
+        f.vrange = float(vrange) if vrange is not None else float(f.x.max() - f.x.min())
         c = self.codecs[0]
         for eb in f.store_bounds:
             s = c.store(f.x, eb)
@@ -93,21 +127,81 @@ class Server:
             f.stored_bytes.append(s.numel())
             self.mem_used += s.numel()
         self.fields[name] = f
+        self._make_room(0, protect_fields={name}, protect_clients=set())
 
-    def _recon(self, client, fname):
+    def _on(self, stream):
+        """Context that makes `stream` current (no-op for a host device)."""
+        if self.dev.type != "cuda":
+            return contextlib.nullcontext()
+        return torch.cuda.stream(stream or torch.cuda.current_stream(self.dev))
+
+    def _spill_root(self) -> str:
+        if self.spill_dir is None:
+            self.spill_dir = tempfile.mkdtemp(prefix="cortado_spill_")
+        os.makedirs(self.spill_dir, exist_ok=True)
+        return self.spill_dir
+
+    def _spill_field(self, f: Field):
+        """Writes the field's stored streams as a storage directory and frees
+        them on the device."""
+        d = os.path.join(self._spill_root(), "fields", f.name)
+        storage.write_storage(d, f.name, [t.cpu().numpy() for t in f.stored], f.store_bounds, f.vrange)
+        f.stored = []
+        f.spilled = d
+        self.mem_used -= f.stored_total
+        self.spills += 1
+
+    def _reload_field(self, f: Field, stream):
+        meta = storage.read_storage_meta(f.spilled)
+        assert [float(e) for e in meta.ebs] == [float(np.float32(e)) for e in f.store_bounds]
+        with self._on(stream):
+            for i, nb in enumerate(f.stored_bytes):
+                h = np.fromfile(os.path.join(f.spilled, storage.stor_name(f.name, i)), dtype=np.uint8)
+                assert h.size == nb
+                f.stored.append(torch.from_numpy(h).to(self.dev))
+        f.spilled = None
+        self.mem_used += f.stored_total
+        self.reloads += 1
+
+    def _spill_client(self, key, st):
+        f = self.fields[key[1]]
+        if st["bound"] is not None:  # a client with progress: its floats are its state
+            path = os.path.join(self._spill_root(), "clients", f"c{key[0]}_{key[1]}.f32")
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            st["recon"].cpu().numpy().tofile(path)
+            st["spilled"] = path
+        st["recon"] = None
+        self.mem_used -= f.n_bytes
+        self.spills += 1
+
+    def _recon(self, client, fname, stream=None, reload=True):
+        """The client's reconstruction of a field, allocated (and counted) if
+        it has none resident; reload=True reads a spilled one back."""
         key = (client, fname)
         st = self.clients.get(key)
         if st is None:
-            f = self.fields[fname]
-            st = {"recon": torch.empty(f.x.numel(), dtype=torch.float32, device=self.dev), "bound": None}
+            st = {"recon": None, "bound": None, "spilled": None, "last_use": 0}
             self.clients[key] = st
+        if st["recon"] is None:
+            f = self.fields[fname]
+            with self._on(stream):
+                st["recon"] = torch.empty(f.x.numel(), dtype=torch.float32, device=self.dev)
+                if reload and st["spilled"]:
+                    st["recon"].copy_(torch.from_numpy(np.fromfile(st["spilled"], dtype=np.float32)))
+                    self.reloads += 1
+            st["spilled"] = None
             self.mem_used += f.n_bytes
         return st
+
+    def _resident(self, key) -> bool:
+        st = self.clients.get(key)
+        return st is not None and st["recon"] is not None
 
     def _out_buffer(self, f: Field) -> torch.Tensor:
         free = self._free_out.get(f.name)
         if free:
             return free.pop()
+        self.mem_used += max_stream_bytes(f.n_bytes)
         return torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
 
     def _stored_for(self, f: Field, bound):
@@ -115,6 +209,44 @@ class Server:
         if i < 0:
             raise ValueError(f"bound {bound} is tighter than every stored bound of {f.name}")
         return f.stored[i]
+
+    # ---------------------------------------------------------------- memory
+    def _make_room(self, need, protect_fields, protect_clients, keep_pool=None) -> bool:
+        """Frees idle state until mem_used + need fits the cap: pooled output
+        buffers (all but keep_pool[field] of each field's), then idle clients'
+        reconstructions, then idle fields' stored streams, least recently used
+        first.  Returns whether it fits."""
+        keep_pool = keep_pool or {}
+        if self.mem_used + need <= self.mem_cap:
+            return True
+        for name, pool in self._free_out.items():
+            keep = keep_pool.get(name, 0)
+            while len(pool) > keep and self.mem_used + need > self.mem_cap:
+                pool.pop()
+                self.mem_used -= max_stream_bytes(self.fields[name].n_bytes)
+        idle = sorted(((st["last_use"], key) for key, st in self.clients.items()
+                       if st["recon"] is not None and key not in protect_clients), key=lambda t: t[0])
+        for _, key in idle:
+            if self.mem_used + need <= self.mem_cap:
+                break
+            self._spill_client(key, self.clients[key])
+        idle_f = sorted(((f.last_use, f.name) for f in self.fields.values()
+                         if f.spilled is None and f.name not in protect_fields), key=lambda t: t[0])
+        for _, name in idle_f:
+            if self.mem_used + need <= self.mem_cap:
+                break
+            self._spill_field(self.fields[name])
+        return self.mem_used + need <= self.mem_cap
+
+    def _materialize(self, reqs, stream):
+        """Makes the state the requests use resident (reads spilled fields and
+        reconstructions back on `stream`; an init's reconstruction is only
+        allocated, its old contents are not needed)."""
+        for r in reqs:
+            f = self.fields[r.field]
+            if f.spilled is not None:
+                self._reload_field(f, stream)
+            self._recon(r.client, r.field, stream, reload=r.kind == "resi")
 
     # ---------------------------------------------------------------- batches
     def _launch(self, k, reqs):
@@ -131,7 +263,7 @@ class Server:
         items_send, items_recv = [], []
         for r in inits:
             f = self.fields[r.field]
-            st = self._recon(r.client, r.field)
+            st = self._recon(r.client, r.field, s)
             out = self._out_buffer(f)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
@@ -146,7 +278,7 @@ class Server:
         items_send, items_recv = [], []
         for r in resis:
             f = self.fields[r.field]
-            st = self._recon(r.client, r.field)
+            st = self._recon(r.client, r.field, s)
             if st["bound"] is None:
                 raise ValueError(f"request {r.rid}: residual before init")
             out = self._out_buffer(f)
@@ -169,7 +301,7 @@ class Server:
     def run(self, requests: list[Request], keep_outputs=False):
         """Serves the trace with continuous batching; returns stats."""
         pending = sorted(requests, key=lambda r: r.arrival)
-        inflight = []          # (event, reqs, outs, sizes, bytes, stream index)
+        inflight = []          # (event, reqs, outs, sizes, stream index)
         waiting = []           # arrived, not yet admitted, in arrival order
         busy_clients = set()
         outputs = {}
@@ -181,18 +313,18 @@ class Server:
             # completions
             still = []
             for item in inflight:
-                ev, reqs, outs, sizes, nbytes, _ = item
+                ev, reqs, outs, sizes, _ = item
                 if ev.query():
                     tdone = time.perf_counter() - t0
                     for r in reqs:
                         r.done = tdone
                         busy_clients.discard((r.client, r.field))
                     for r in reqs:
-                        if keep_outputs:  # handed to the caller, not reused
+                        if keep_outputs:  # handed to the caller, no longer counted
                             outputs[r.rid] = outs[r.rid]
+                            self.mem_used -= max_stream_bytes(self.fields[r.field].n_bytes)
                         else:
                             self._free_out.setdefault(r.field, []).append(outs[r.rid])
-                    self.mem_used -= nbytes
                 else:
                     still.append(item)
             inflight = still
@@ -202,10 +334,12 @@ class Server:
             while i < len(pending) and pending[i].arrival <= now:
                 waiting.append(pending[i])
                 i += 1
-            batch, nbytes = [], 0
+            batch = []
             room = min(self.max_batch, self.max_inflight - sum(len(x[1]) for x in inflight))
             if room > 0 and waiting:
                 held, keep = set(), []
+                need_total, claims, new_recons, reloads = 0, {}, set(), set()
+                busy_fields = {r.field for x in inflight for r in x[1]}
                 for j, r in enumerate(waiting):
                     if len(batch) >= room:
                         keep.extend(waiting[j:])
@@ -215,22 +349,45 @@ class Server:
                         held.add(key)
                         keep.append(r)
                         continue
-                    need = max_stream_bytes(self.fields[r.field].n_bytes)
-                    if self.mem_used + nbytes + need > self.mem_cap:
-                        keep.extend(waiting[j:])
-                        break
+                    f = self.fields[r.field]
+                    pooled = len(self._free_out.get(r.field, ())) > claims.get(r.field, 0)
+                    need = 0 if pooled else max_stream_bytes(f.n_bytes)
+                    if f.spilled is not None and r.field not in reloads:
+                        need += f.stored_total
+                    if not self._resident(key) and key not in new_recons:
+                        need += f.n_bytes
+                    if self.mem_used + need_total + need > self.mem_cap:
+                        protect_f = busy_fields | {b.field for b in batch} | {r.field}
+                        protect_c = busy_clients | {key}
+                        keep_pool = dict(claims)
+                        if pooled:  # the buffer this request will take stays
+                            keep_pool[r.field] = keep_pool.get(r.field, 0) + 1
+                        if not self._make_room(need_total + need, protect_f, protect_c, keep_pool):
+                            keep.extend(waiting[j:])
+                            break
                     batch.append(r)
                     busy_clients.add(key)
-                    nbytes += need
+                    need_total += need
+                    if pooled:
+                        claims[r.field] = claims.get(r.field, 0) + 1
+                    if f.spilled is not None:
+                        reloads.add(r.field)
+                    if not self._resident(key):
+                        new_recons.add(key)
                 waiting = keep
             if batch:
-                self.mem_used += nbytes
+                self._tick += 1
+                for r in batch:
+                    self.fields[r.field].last_use = self._tick
+                self._materialize(batch, self.streams[k])
+                for r in batch:
+                    self.clients[(r.client, r.field)]["last_use"] = self._tick
                 ev, outs, sizes = self._launch(k, batch)
-                inflight.append((ev, batch, outs, sizes, nbytes, k))
+                inflight.append((ev, batch, outs, sizes, k))
                 k = (k + 1) % len(self.streams)
             elif inflight:
                 time.sleep(20e-6)
-            elif waiting:
+            elif waiting:  # the head cannot fit even with nothing in flight
                 raise RuntimeError(f"request {waiting[0].rid} needs more than the {self.mem_cap}-byte memory cap")
             elif i < len(pending):
                 time.sleep(max(0.0, min(1e-3, pending[i].arrival - (time.perf_counter() - t0))))
@@ -255,7 +412,16 @@ class Server:
             if r.arrival > now:
                 time.sleep(r.arrival - now)
             f = self.fields[r.field]
-            st = self._recon(r.client, r.field)
+            key = (r.client, r.field)
+            need = max_stream_bytes(f.n_bytes) + (f.stored_total if f.spilled else 0) + \
+                (0 if self._resident(key) else f.n_bytes)
+            if not self._make_room(need, {r.field}, {key}):
+                raise RuntimeError(f"request {r.rid} needs more than the {self.mem_cap}-byte memory cap")
+            self._tick += 1
+            f.last_use = self._tick
+            self._materialize([r], s)
+            st = self.clients[key]
+            st["last_use"] = self._tick
             stored = self._stored_for(f, r.bound)
             with torch.cuda.stream(s):
                 out = torch.empty(max_stream_bytes(f.n_bytes), dtype=torch.uint8, device=self.dev)
@@ -278,15 +444,20 @@ class Server:
         orig = sum(self.fields[r.field].n_bytes for r in requests if r.done >= 0)
         return {"requests": len(lat), "wall_s": wall, "orig_GBps": orig * 1e-9 / wall if wall > 0 else None,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3) if lat.size else None,
-                "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else None}
+                "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else None,
+                "spills": self.spills, "reloads": self.reloads}
 
     def prepare(self, requests: list[Request]):
         """Allocates the reconstruction of every (client, field) the requests
-        touch, as a server does when a client opens a field, and sizes every
-        context's scratch for the largest batch (max_batch requests on the
-        largest field), so that serving itself allocates only output streams."""
+        touch, as a server does when a client opens a field, while they fit
+        under the memory cap (the others are allocated at admission), and
+        sizes every context's scratch for the largest batch (max_batch
+        requests on the largest field), so that serving itself allocates
+        only output streams."""
         for r in requests:
-            self._recon(r.client, r.field)
+            key = (r.client, r.field)
+            if not self._resident(key) and self.mem_used + self.fields[r.field].n_bytes <= self.mem_cap:
+                self._recon(r.client, r.field)
         if self.fields:
             chunks = max(-(-f.n_bytes // 16384) for f in self.fields.values())
             for c in self.codecs:
@@ -298,9 +469,11 @@ class Server:
         if not free:
             for st in self.clients.values():
                 st["bound"] = None
+                st["spilled"] = None
             return
         for (c, fname), st in self.clients.items():
-            self.mem_used -= self.fields[fname].n_bytes
+            if st["recon"] is not None:
+                self.mem_used -= self.fields[fname].n_bytes
         self.clients.clear()
 
     def close(self):

@@ -66,3 +66,40 @@ def test_served_results_equal_alone(cuda_device, backlog, max_batch):
         assert O.maxabs(v["recon"].cpu().numpy(), x.cpu().numpy(), v["bound"]) == -1
     assert stats_b["p50_ms"] is not None and stats_b["p99_ms"] >= stats_b["p50_ms"]
     srv.close()
+
+
+def test_memory_cap_spills_and_reloads_with_identical_results(cuda_device, tmp_path):
+    """A cap below the working set: idle reconstructions and stored fields are
+    spilled to host files and read back; every request's stream and every
+    final reconstruction equal those of a server without the cap."""
+    from cortado_b200.ops import max_stream_bytes
+    from cortado_b200.serve import Server, poisson_trace
+    big, ranges = _server(cuda_device.index, max_batch=4)
+    rng = np.random.Generator(np.random.PCG64(23))
+    trace = poisson_trace(rng, big.fields, 40, rate_hz=20000.0, n_clients=4, ranges=ranges)
+    for r in trace:
+        r.arrival = 0.0
+    _, out_big = big.run(trace, keep_outputs=True)
+    recon_big = {k: v["recon"].clone() for k, v in big.clients.items()}
+    # room for the largest field's stored streams plus four output buffers and
+    # four reconstructions of the largest field
+    nmax = max(f.n_bytes for f in big.fields.values())
+    cap = max(f.stored_total for f in big.fields.values()) + 4 * (max_stream_bytes(nmax) + nmax)
+    small = Server(cuda_device.index, mem_cap_bytes=cap, max_inflight=16, n_streams=3, max_batch=4,
+                   spill_dir=str(tmp_path))
+    for name, f in big.fields.items():
+        small.add_field(name, f.x, f.store_bounds, vrange=ranges[name])
+    for r in trace:
+        r.done = -1.0
+    stats, out_small = small.run(trace, keep_outputs=True)
+    assert stats["requests"] == len(trace) and stats["spills"] > 0 and stats["reloads"] > 0
+    for r in trace:
+        a, b = out_small[r.rid], out_big[r.rid]
+        n = _stream_len(b)
+        assert _stream_len(a) == n and torch.equal(a[:n], b[:n]), r
+    for k, v in recon_big.items():
+        st = small.clients[k]
+        got = st["recon"] if st["recon"] is not None else torch.from_numpy(np.fromfile(st["spilled"], np.float32))
+        assert torch.equal(got.cpu().view(torch.int32), v.cpu().view(torch.int32)), k
+    small.close()
+    big.close()
