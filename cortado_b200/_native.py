@@ -40,9 +40,12 @@ SIGNATURES = {
     "cortado_set_launch_ctas": (_int, [_vp, _int, _int]),
     "cortado_reserve": (_int, [_vp, _i64, _int]),
     "cortado_selftest_timeout": (_int, [_vp, _vp]),
+    "cortado_init_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _vp, _i64, _vp, _vp, _vp]),
+    "cortado_resi_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _f32, _vp, _i64, _vp, _vp, _vp]),
 }
 
-OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5}
+OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5,
+       "init_send_apply": 6, "resi_send_apply": 7}
 
 
 class Item(ctypes.Structure):

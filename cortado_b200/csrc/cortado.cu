@@ -18,7 +18,9 @@ using namespace cortado;
 // ================================================================== kernels
 // Resident CTAs per SM each kernel is compiled for (register budget
 // 65536 / (128 * n)); every kernel holds two 17 KiB buffers, so shared memory
-// allows 6.
+// allows 6.  resi_recv runs 5 (102 registers): at 80 its client and residual
+// words spill, and it measured 4.6% faster at 5; every other kernel measured
+// slower at 5 (and the store 10% slower with a third buffer at 4).
 #ifndef MINB_STORE
 #define MINB_STORE 6
 #endif
@@ -29,7 +31,7 @@ using namespace cortado;
 #define MINB_DEC 6
 #endif
 #ifndef MINB_RAPPLY
-#define MINB_RAPPLY 6
+#define MINB_RAPPLY 5
 #endif
 
 namespace {
@@ -497,6 +499,61 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
   flush_pending(sm, src, s ^ 1, B, raw_word);
 }
 
+// The client side of a served request, fused into init_send / resi_send
+// (cortado_*_send_apply): the words the re-encoder is about to encode (request
+// bins, or residuals) are applied to the client's reconstruction directly,
+// so the stream just written need not be decoded again.  The results equal
+// init_recv / resi_recv of that stream bit for bit:
+//   init: iCQ(bin) (d_client_encode.h:230-254); a chunk that the encoder
+//         stores uncompressed is rewritten with its bins afterwards
+//         (client_raw_bins), as init_recv copies raw chunks out as stored;
+//   resi: iCQ(CQ(client, dst) + residual, dst) (d_RESI_4.h:79-94); the
+//         residual ints are the same whether the chunk compresses or not.
+// Thread g handles its group's 32 words, 16 bytes at a time (the client's
+// words are read and written in place); forms as in the decoders, chosen per
+// word.
+template <int OP>
+__device__ __forceinline__ void client_apply(const OpArgs& A, long long c, int nw, const uint32_t (&v)[32], Quant q) {
+  const int tid = threadIdx.x;
+  const FastQ fq = make_fastq(q.eb_e);
+  uint32_t* row = reinterpret_cast<uint32_t*>(A.client) + c * (long long)CW + 32 * tid;
+  if (nw == CW) {
+    uint4* r4 = reinterpret_cast<uint4*>(row);
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      uint4 o;
+      if (OP == OP_S2C) {
+        o = make_uint4(iq_mixed(v[4 * u], fq, q), iq_mixed(v[4 * u + 1], fq, q), iq_mixed(v[4 * u + 2], fq, q),
+                       iq_mixed(v[4 * u + 3], fq, q));
+      } else {
+        const uint4 w = r4[u];
+        o = make_uint4(iq_mixed(cq_mixed(w.x, fq, q) + v[4 * u], fq, q),
+                       iq_mixed(cq_mixed(w.y, fq, q) + v[4 * u + 1], fq, q),
+                       iq_mixed(cq_mixed(w.z, fq, q) + v[4 * u + 2], fq, q),
+                       iq_mixed(cq_mixed(w.w, fq, q) + v[4 * u + 3], fq, q));
+      }
+      r4[u] = o;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      if (32 * tid + k < nw) {
+        row[k] = (OP == OP_S2C) ? iq_mixed(v[k], fq, q) : iq_mixed(cq_mixed(row[k], fq, q) + v[k], fq, q);
+      }
+    }
+  }
+}
+
+// init_send with apply, for a chunk stored uncompressed: its bins (rebuilt
+// into row tid of Yw by raw_rebuild) replace the dequantized words this
+// thread wrote, as init_recv emits a raw chunk's bins unchanged.
+__device__ __noinline__ void client_raw_bins(const OpArgs& A, long long c, int nw, const uint32_t* Yw) {
+  const int tid = threadIdx.x;
+  uint32_t* row = reinterpret_cast<uint32_t*>(A.client) + c * (long long)CW + 32 * tid;
+  for (int k = 0; k < 32; k++)
+    if (32 * tid + k < nw) row[k] = Yw[swz(32 * tid + k)];
+}
+
 // Rebuilds a raw chunk's requantized words from the plane buffer into the
 // staging buffer (out of line: only chunks that do not compress take it, and
 // the re-encoders' loop is large enough to stall on instruction fetch).
@@ -537,6 +594,14 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       long long g = 0;
       if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
       prefetch_stream(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
+      if (OP == OP_RESI && lane == 0) {
+        // resi_send with apply reads the client's chunk: bring it into L2 now
+        const StageMeta& mn = sm.st[0];
+        if (mn.g < src.total && mn.bad == 0) {
+          const OpArgs& An = src.args(mn.item);
+          if (An.client && mn.nw == CW) prefetch_l2(An.client + mn.c * (long long)CS, CS);
+        }
+      }
     }
   };
   take_next();
@@ -607,6 +672,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
         row_load(X, tid, v);
       }
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
+      if (A.client) client_apply<OP>(A, c, nw, v, OP == OP_S2C ? q1 : q2);
       if (nw == CW) {
         encode_stage<true>(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s], flush_prev);
       } else {
@@ -618,6 +684,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       if (sm.pend[s].raw) {
         // the requantized words, rebuilt from the plane buffer, are the payload
         raw_rebuild(sm, X, nw, Yw);
+        if (OP == OP_S2C && A.client) client_raw_bins(A, c, nw, Yw);
       }
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
@@ -1307,10 +1374,10 @@ cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t 
 
 static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
                                float eb1, float eb2, void* d_out, int64_t out_capacity, int64_t* d_outsize,
-                               cortado_stream_t stream) {
+                               cortado_stream_t stream, void* d_client = nullptr) {
   if (!ctx || !d_stored || !d_out || !d_outsize || n_bytes < 0 || (n_bytes & 3) || stored_bytes < HDR)
     return CORTADO_ERR_INVALID_ARG;
-  if (!aligned16(d_stored) || !aligned16(d_out)) return CORTADO_ERR_ALIGNMENT;
+  if (!aligned16(d_stored) || !aligned16(d_out) || (d_client && !aligned16(d_client))) return CORTADO_ERR_ALIGNMENT;
   if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
   int e1 = 0, e2 = 0;
   cortado_status s = eb_exponent(eb1, &e1);
@@ -1328,6 +1395,7 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.n = n_bytes;
   a.q1 = make_quant(e1);
   a.q2 = make_quant(e2);
+  a.client = (uint8_t*)d_client;
   a.sy = next_sync(ctx, st);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
   if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
@@ -1346,6 +1414,22 @@ cortado_status cortado_resi_send(cortado_ctx* ctx, const void* d_stored, int64_t
                                  int64_t* d_outsize, cortado_stream_t stream) {
   return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_abs, dst_eb_abs, d_out, out_capacity, d_outsize,
                   stream);
+}
+
+cortado_status cortado_init_send_apply(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                       float request_eb_abs, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                       void* d_client, cortado_stream_t stream) {
+  if (!d_client && n_bytes) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_S2C, d_stored, stored_bytes, n_bytes, request_eb_abs, 0.0f, d_out, out_capacity, d_outsize,
+                  stream, d_client);
+}
+
+cortado_status cortado_resi_send_apply(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                       float src_eb_abs, float dst_eb_abs, void* d_out, int64_t out_capacity,
+                                       int64_t* d_outsize, void* d_client, cortado_stream_t stream) {
+  if (!d_client && n_bytes) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_abs, dst_eb_abs, d_out, out_capacity, d_outsize,
+                  stream, d_client);
 }
 
 static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int64_t stream_bytes, const void* d_src,
@@ -1439,7 +1523,10 @@ cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_b
 
 cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item* items, int n_items,
                              cortado_stream_t stream) {
-  if (!ctx || !items || n_items <= 0 || op < CORTADO_OP_STORE || op > CORTADO_OP_RESI_RECV) return CORTADO_ERR_INVALID_ARG;
+  if (!ctx || !items || n_items <= 0 || op < CORTADO_OP_STORE || op > CORTADO_OP_RESI_SEND_APPLY) return CORTADO_ERR_INVALID_ARG;
+  // the fused send-and-apply forms run the re-encoders with the client's floats
+  const bool apply = op == CORTADO_OP_INIT_SEND_APPLY || op == CORTADO_OP_RESI_SEND_APPLY;
+  if (apply) op = (op == CORTADO_OP_INIT_SEND_APPLY) ? CORTADO_OP_INIT_SEND : CORTADO_OP_RESI_SEND;
   static_assert((int)CORTADO_OP_STORE == OP_STORE && (int)CORTADO_OP_INIT_SEND == OP_S2C &&
                     (int)CORTADO_OP_RESI_SEND == OP_RESI && (int)CORTADO_OP_STORE_DECODE == OP_SDEC &&
                     (int)CORTADO_OP_INIT_RECV == OP_CDEC && (int)CORTADO_OP_RESI_RECV == OP_RAPPLY,
@@ -1461,7 +1548,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
         break;
       case CORTADO_OP_INIT_SEND:
       case CORTADO_OP_RESI_SEND:
-        if (it.in_bytes < HDR) return CORTADO_ERR_INVALID_ARG;
+        if (it.in_bytes < HDR || (apply && !it.d_src)) return CORTADO_ERR_INVALID_ARG;
         if (it.out_capacity < cortado_max_stream_bytes(it.n_bytes)) return CORTADO_ERR_CAPACITY;
         if ((s = eb_exponent(it.eb1, &e))) return s;
         if (op == CORTADO_OP_RESI_SEND && (s = eb_exponent(it.eb2, &e))) return s;
@@ -1504,6 +1591,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
     eb_exponent(it.eb2, &e2);
     a.q1 = make_quant(e1);
     a.q2 = make_quant(e2);
+    a.client = apply ? (uint8_t*)it.d_src : nullptr;
     a.sy = sy;
     a.sy.flags = sy.flags + base;
     a.sy.offs = sy.offs + base;

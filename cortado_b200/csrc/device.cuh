@@ -147,6 +147,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
+// L2 prefetch of `bytes` (a multiple of 16) at a 16-byte-aligned address.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // ---------------------------------------------------------------- status
 __device__ __forceinline__ void latch(unsigned int* status, unsigned int code) {
   atomicCAS(status, 0u, code);

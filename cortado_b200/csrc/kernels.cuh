@@ -30,6 +30,7 @@ struct OpArgs {
   Quant q1, q2;             // store: server; init_send: request; resi_send: src, dst
   Sync sy;
   int has_map_in, has_map_out;
+  uint8_t* client;          // init_send / resi_send with apply: the client's reconstruction (floats), or null
 };
 
 // ---------------------------------------------------------------- shared memory

@@ -136,6 +136,26 @@ class Codec:
         check(self._L.cortado_resi_recv(self._h, _ptr(d_src), int(srcsize), _ptr(d_residual), n, _ptr(d_dest),
                                         _nbytes(d_dest), _ptr(d_destsize), _stream(stream)), "residual_apply")
 
+    def s2c_encode_apply(self, d_input, d_output, d_outsize, request_eb, n_bytes, d_client, in_bytes=None,
+                         stream=None):
+        """init_send fused with the client's init_recv: the init stream into
+        d_output and, in the same pass, the client's reconstruction into
+        d_client (as client_decode of that stream would write it)."""
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_init_send_apply(self._h, _ptr(d_input), n, int(n_bytes), float(request_eb),
+                                              _ptr(d_output), _nbytes(d_output), _ptr(d_outsize), _ptr(d_client),
+                                              _stream(stream)), "s2c_encode_apply")
+
+    def residual_encode_apply(self, d_input, d_output, d_outsize, src_eb, dest_eb, n_bytes, d_client, in_bytes=None,
+                              stream=None):
+        """resi_send fused with the client's resi_recv: the residual stream
+        into d_output, and d_client (the client's floats at src_eb) updated in
+        place as residual_apply of that stream would."""
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_resi_send_apply(self._h, _ptr(d_input), n, int(n_bytes), float(src_eb), float(dest_eb),
+                                              _ptr(d_output), _nbytes(d_output), _ptr(d_outsize), _ptr(d_client),
+                                              _stream(stream)), "residual_encode_apply")
+
     def INOA_find_range(self, d_data, size=None, stream=None):
         n = _nbytes(d_data) if size is None else int(size)
         lo, hi = ctypes.c_float(), ctypes.c_float()

@@ -17,7 +17,11 @@ request of the same client on the same field still running or waiting (a
 client's steps are ordered); a request held back for that reason does not hold
 back other clients' requests.  The admitted requests are grouped by operation
 and run as batched launches (``cortado_batch``: one persistent launch per
-operation for the whole group) on one of ``n_streams`` CUDA streams.
+operation for the whole group) on one of ``n_streams`` CUDA streams.  Each
+launch is a send fused with the client's receive (init_send_apply,
+resi_send_apply): it writes the stream that goes to the client and, in the
+same pass, the client's resident reconstruction, exactly as a separate
+receive of that stream would.
 Admission does not wait for earlier batches: a new batch starts on the next
 stream while others are still on the GPU (several batches in flight keep the
 GPU busy while the host assembles the next one), and completions are polled
@@ -115,6 +119,7 @@ class Server:
         # fell back to a fresh cudaMalloc, which stalls the device.)  Pooled
         # buffers count against the memory cap until they are freed.
         self._free_out: dict[str, list[torch.Tensor]] = {}
+        self._timeline = []
 
     # ---------------------------------------------------------------- storage
     def add_field(self, name, x, store_bounds_abs, vrange=None):
@@ -252,6 +257,8 @@ class Server:
     def _launch(self, k, reqs):
         """Enqueues one batch (any mix of init and resi requests) on stream k."""
         codec, s = self.codecs[k], self.streams[k]
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record(s)
         inits = [r for r in reqs if r.kind == "init"]
         resis = [r for r in reqs if r.kind == "resi"]
         # Everything this batch allocates is allocated on its own stream, so the
@@ -260,22 +267,20 @@ class Server:
             sizes = torch.empty(max(1, len(reqs)) * 2, dtype=torch.int64, device=self.dev)
         outs = {}
         j = 0
-        items_send, items_recv = [], []
+        items_send = []
         for r in inits:
             f = self.fields[r.field]
             st = self._recon(r.client, r.field, s)
             out = self._out_buffer(f)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
-                                   n_bytes=f.n_bytes, eb1=r.bound))
-            items_recv.append(dict(**{"in": out}, out=st["recon"], out_size=sizes[j + 1:j + 2], n_bytes=f.n_bytes))
+                                   n_bytes=f.n_bytes, eb1=r.bound, src=st["recon"]))
             st["bound"] = r.bound
             j += 2
         with torch.cuda.stream(s):
-            if items_send:
-                codec.batch("init_send", items_send, stream=s)
-                codec.batch("init_recv", items_recv, stream=s)
-        items_send, items_recv = [], []
+            if items_send:  # init_send with the client's init_recv fused in
+                codec.batch("init_send_apply", items_send, stream=s)
+        items_send = []
         for r in resis:
             f = self.fields[r.field]
             st = self._recon(r.client, r.field, s)
@@ -284,17 +289,15 @@ class Server:
             out = self._out_buffer(f)
             outs[r.rid] = out
             items_send.append(dict(**{"in": self._stored_for(f, r.bound)}, out=out, out_size=sizes[j:j + 1],
-                                   n_bytes=f.n_bytes, eb1=st["bound"], eb2=r.bound))
-            items_recv.append(dict(**{"in": out}, src=st["recon"], out=st["recon"], out_size=sizes[j + 1:j + 2],
-                                   n_bytes=f.n_bytes))
+                                   n_bytes=f.n_bytes, eb1=st["bound"], eb2=r.bound, src=st["recon"]))
             st["bound"] = r.bound
             j += 2
         with torch.cuda.stream(s):
-            if items_send:
-                codec.batch("resi_send", items_send, stream=s)
-                codec.batch("resi_recv", items_recv, stream=s)
-        ev = torch.cuda.Event()
+            if items_send:  # resi_send with the client's resi_recv fused in
+                codec.batch("resi_send_apply", items_send, stream=s)
+        ev = torch.cuda.Event(enable_timing=True)
         ev.record(s)
+        self._timeline.append((ev0, ev))
         return ev, outs, sizes
 
     # ---------------------------------------------------------------- loops
@@ -305,6 +308,11 @@ class Server:
         waiting = []           # arrived, not yet admitted, in arrival order
         busy_clients = set()
         outputs = {}
+        self._timeline = []  # (start, end) events of every batch, on its stream
+        origin = None
+        if self.dev.type == "cuda":
+            origin = torch.cuda.Event(enable_timing=True)
+            origin.record(self.streams[0])
         t0 = time.perf_counter()
         k = 0
         i = 0
@@ -394,7 +402,32 @@ class Server:
         for c, s in zip(self.codecs, self.streams):
             c.sync(s)
         wall = time.perf_counter() - t0
-        return self._stats(requests, wall), outputs
+        st = self._stats(requests, wall)
+        if origin is not None:
+            st.update(self._device_timeline(origin, wall))
+        return st, outputs
+
+    def _device_timeline(self, origin, wall):
+        """Device view of a run from its batches' start and end events: how
+        long the GPU had at least one batch running (the union of the batches'
+        intervals), as a fraction of the run's wall time, and the median
+        batch duration.  Throughput below the device rate with a low busy
+        fraction means the host (or another process) left the GPU idle."""
+        iv = sorted((origin.elapsed_time(a), origin.elapsed_time(b)) for a, b in self._timeline)
+        busy, cur_s, cur_e = 0.0, None, None
+        for a, b in iv:
+            if cur_e is None or a > cur_e:
+                if cur_e is not None:
+                    busy += cur_e - cur_s
+                cur_s, cur_e = a, b
+            else:
+                cur_e = max(cur_e, b)
+        if cur_e is not None:
+            busy += cur_e - cur_s
+        dur = sorted(b - a for a, b in iv)
+        return {"batches": len(iv), "device_busy_ms": busy,
+                "device_busy_frac": busy / (wall * 1e3) if wall > 0 else None,
+                "batch_ms_p50": dur[len(dur) // 2] if dur else None}
 
     def run_plain(self, requests: list[Request], keep_outputs=False):
         """The plain per-request pipeline: requests in arrival order, each as

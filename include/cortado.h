@@ -113,6 +113,26 @@ cortado_status cortado_resi_recv(cortado_ctx* ctx, const void* d_src, int64_t n_
                                  int64_t resi_bytes, void* d_out, int64_t out_capacity, int64_t* d_outsize,
                                  cortado_stream_t stream);
 
+/* init_send fused with the client's init_recv, for a server that holds the
+ * client's reconstruction on the same device (a serving loop).  Writes the
+ * init stream exactly as cortado_init_send() does and, in the same pass,
+ * d_client (n_bytes of floats) exactly as cortado_init_recv() of that stream
+ * would, without decoding it again.  No single counterpart in the reference:
+ * it replaces d_s2c_encode (include/d_s2c.h:203-224) followed by
+ * d_client_decode (include/d_client_encode.h:262-266). */
+cortado_status cortado_init_send_apply(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                       float request_eb_abs, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                       void* d_client, cortado_stream_t stream);
+
+/* resi_send fused with the client's resi_recv: writes the residual stream as
+ * cortado_resi_send() does and updates d_client (the client's floats at the
+ * source bound, n_bytes) in place to what cortado_resi_recv() of that stream
+ * would produce.  Replaces d_residual_encode (include/d_residual_encode.h:204-230)
+ * followed by d_residual_apply (include/d_residual_encode.h:350-354). */
+cortado_status cortado_resi_send_apply(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                       float src_eb_abs, float dst_eb_abs, void* d_out, int64_t out_capacity,
+                                       int64_t* d_outsize, void* d_client, cortado_stream_t stream);
+
 /* NOA range: min and max of the floats (NaNs ignored), synchronous.
  * Replaces d_INOA_find_range, include/preprocessors/include/INOA_f32.h:52-61. */
 cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
@@ -138,7 +158,9 @@ typedef enum {
   CORTADO_OP_RESI_SEND = 2,    /* d_in: stored stream, eb1: source, eb2: destination bound */
   CORTADO_OP_STORE_DECODE = 3, /* d_in: stored stream */
   CORTADO_OP_INIT_RECV = 4,    /* d_in: init stream */
-  CORTADO_OP_RESI_RECV = 5     /* d_in: residual stream, d_src: the client's floats */
+  CORTADO_OP_RESI_RECV = 5,    /* d_in: residual stream, d_src: the client's floats */
+  CORTADO_OP_INIT_SEND_APPLY = 6, /* as INIT_SEND, and d_src: the client's floats, written (init_send_apply) */
+  CORTADO_OP_RESI_SEND_APPLY = 7  /* as RESI_SEND, and d_src: the client's floats, updated (resi_send_apply) */
 } cortado_op;
 
 typedef struct {
