@@ -181,11 +181,19 @@ def run_gpu(args, rank, world):
 
 
 def _run_gpu(args, rank, world):
-    from cortado_b200 import ops
+    import tempfile
+    from cortado_b200 import autotune, ops
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    codec = ops.Codec(dev.index)
     x = make_field(2 + rank, dev, args.shape)
+    # The autotuner picks every operation's launch parameters on this GPU for
+    # the workload's size class (untimed, before the warm-up), into a cache
+    # private to this run that every later context of the process applies.
+    os.environ["CORTADO_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="cortado_tune_"), "tune.json")
+    codec = ops.Codec(dev.index)
+    tuning = autotune.tune(codec, n_bytes=x.numel() * 4) if not args.no_tune else None
+    if tuning is not None:
+        autotune.save_cache({autotune.key(dev, x.numel() * 4): tuning})
     stream = torch.cuda.Stream(dev)
     fl = Flow(codec, x, stream)
     with torch.cuda.stream(stream):
@@ -317,7 +325,7 @@ def _run_gpu(args, rank, world):
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = reference_cuda_baseline(x_host)
     return dict(abs=abs_res, ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
-                h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda)
+                h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda, tuning=tuning)
 
 
 def barrier(world):
@@ -598,6 +606,7 @@ def main():
     ap.add_argument("--cpu-sample-mb", type=int, default=0,
                     help="CPU legs on a smaller field of about this many MiB (0: the whole field)")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA build")
+    ap.add_argument("--no-tune", action="store_true", help="keep the shipped launch parameters (no tuning run)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="512,512,512", help="field shape (profiling uses a smaller one)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
@@ -672,6 +681,10 @@ def main():
                              for k, t in zip(OPS, r["abs"]["per_op"])}},
         "clocks": r["clocks"],
     }
+    if r["tuning"] is not None:
+        line["tuning"] = {"source": "tuned on this GPU for the workload's size class before the warm-up",
+                          "params": {op: {k: v[k] for k in ("ctas_per_sm", "resolver")} for op, v in r["tuning"].items()},
+                          "sweep_ms": {op: v["sweep_ms"] for op, v in r["tuning"].items()}}
     if r["ref_cuda"] is not None:
         rc = r["ref_cuda"]
         if "noa" in rc:  # set beside this run's own per-operation times

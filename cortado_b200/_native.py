@@ -38,6 +38,7 @@ SIGNATURES = {
     "cortado_batch": (_int, [_vp, _int, _vp, _int, _vp]),
     "cortado_verify_bound": (_int, [_vp, _vp, _vp, _i64, _f32, _vp, _vp]),
     "cortado_set_launch_ctas": (_int, [_vp, _int, _int]),
+    "cortado_set_resolver": (_int, [_vp, _int, _int]),
     "cortado_reserve": (_int, [_vp, _i64, _int]),
     "cortado_selftest_timeout": (_int, [_vp, _vp]),
     "cortado_init_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _vp, _i64, _vp, _vp, _vp]),

@@ -1,17 +1,27 @@
 """Autotuner for the processing parameters of the encode/decode kernels.
 
-The chunk size (16 KiB) is a format constant: changing it would change every
-stream, so it is not tuned.  Threads per chunk (128) is fixed by the kernels'
-register layout.  What varies at run time, and what this module tunes, is the
-persistent grid of each operation: how many CTAs per SM are resident. That
-trades latency hiding against shared-memory and L2 pressure.  The choice never
-changes output bytes.
+Only parameters that change speed, never output bytes, are tuned:
 
-``tune(codec, ...)`` sweeps CTAs per SM for each operation on a seeded
-synthetic field of the given size class and keeps the fastest. Results are
-cached in a JSON file keyed by GPU name and size class.  ``apply(codec, ...)``
-loads the cached choice (tuning on a miss) and sets it on the context with
-``cortado_set_launch_ctas``.
+* CTAs per SM of each operation's persistent grid (``cortado_set_launch_ctas``;
+  the batched launches of an operation use the same setting): latency hiding
+  against shared-memory and L2 pressure;
+* for the three encoders, whether the helper CTA's resolver warp turns
+  published chunk sizes into inclusive prefixes ahead of the flushes
+  (``cortado_set_resolver``), or each flush walks the lookback words itself.
+
+Not tuned, because they are fixed by the format or the register layout: the
+chunk size (16 KiB, part of every stream), threads per chunk (128: one
+32-word group per thread), and the lookback window (32 words, one per lane;
+wider windows measured slower and need a different register layout).
+
+``tune(codec, n_bytes)`` sweeps the parameters per operation on the
+benchmark's kind of field (seeded sinusoid with 0.1% outliers, NOA flow) of
+the given size and keeps the fastest; results are keyed by GPU name and size
+class.  ``apply(codec, n_bytes)`` sets the chosen parameters on a context:
+from the user cache (``CORTADO_TUNE_CACHE`` or ~/.cache/cortado_b200), else
+from the table shipped for the GPU (``cortado_b200/tuning/*.json``), else the
+built-in defaults; it tunes only when asked (``tune_on_miss``).  Codec
+creation applies the table for the default size class.
 """
 from __future__ import annotations
 
@@ -25,12 +35,14 @@ from . import fields, storage
 from .ops import Codec, max_stream_bytes
 
 OPS = ("store", "init_send", "init_recv", "resi_send", "resi_recv")
+ENCODERS = ("store", "init_send", "resi_send")
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_CLASS = "le512MiB"
 
 
 def cache_path() -> str:
-    base = os.environ.get("CORTADO_TUNE_CACHE") or os.path.join(
+    return os.environ.get("CORTADO_TUNE_CACHE") or os.path.join(
         os.environ.get("XDG_CACHE_HOME", os.path.expanduser("~/.cache")), "cortado_b200", "tune.json")
-    return base
 
 
 def size_class(n_bytes: int) -> str:
@@ -41,8 +53,17 @@ def size_class(n_bytes: int) -> str:
     return "gt512MiB"
 
 
-def _key(codec: Codec, n_bytes: int) -> str:
-    return f"{torch.cuda.get_device_name(codec.device)}|{size_class(n_bytes)}"
+def gpu_name(device) -> str:
+    return torch.cuda.get_device_name(device)
+
+
+def key(device, n_bytes: int) -> str:
+    return f"{gpu_name(device)}|{size_class(n_bytes)}"
+
+
+def shipped_path(device) -> str:
+    name = "".join(ch if ch.isalnum() else "_" for ch in gpu_name(device))
+    return os.path.join(HERE, "tuning", name + ".json")
 
 
 def _time(fn, reps):
@@ -59,11 +80,22 @@ def _time(fn, reps):
     return statistics.median(ts)
 
 
-def tune(codec: Codec, n_bytes: int = 64 << 20, candidates=(2, 3, 4, 5, 6), reps: int = 5) -> dict:
-    """Sweeps CTAs per SM per operation on a sinusoid field of n_bytes at
-    NOA 1e-4 (store), 1e-2 (init), 1e-2 -> 1e-4 (residual)."""
+def set_params(codec: Codec, params: dict) -> None:
+    """Applies {op: {"ctas_per_sm": n, "resolver": 0/1}} to a context."""
+    for op, v in params.items():
+        codec.set_launch_ctas(op, int(v.get("ctas_per_sm", 0)))
+        if op in ENCODERS and "resolver" in v:
+            codec.set_resolver(op, bool(v["resolver"]))
+
+
+def tune(codec: Codec, n_bytes: int = 128 << 20, ctas=(3, 4, 5, 6), reps: int = 5) -> dict:
+    """Sweeps every operation's parameters on a seeded sinusoid + 0.1%
+    outliers field of n_bytes at NOA 1e-4 (store), 1e-2 (init) and
+    1e-2 -> 1e-4 (residual); returns {op: {"ctas_per_sm", "resolver", "ms",
+    "sweep_ms"}} and leaves the best setting applied."""
     dev = codec.device
-    x = fields.mixed_field(n_bytes // 4, "sinusoid", 7, device=dev)
+    side = max(1, n_bytes // (4 * 512 * 512))
+    x = fields.sinusoid((side, 512, 512), 2, outlier_frac=1e-3, device=dev).reshape(-1)
     n = x.numel() * 4
     lo, hi = codec.INOA_find_range(x)
     rng = storage.value_range(lo, hi)
@@ -79,29 +111,36 @@ def tune(codec: Codec, n_bytes: int = 64 << 20, candidates=(2, 3, 4, 5, 6), reps
         "resi_send": lambda: codec.residual_encode(stor, resi, sz[3:4], eb_i, eb_d, n),
         "resi_recv": lambda: codec.residual_apply(cl, n, resi, fin, sz[4:5]),
     }
-    for op in OPS:  # produce valid inputs for every later op
+    for op in OPS:  # valid inputs for every later op
         calls[op]()
     codec.sync()
     best = {}
     for op in OPS:
         results = {}
-        for c in candidates:
-            codec.set_launch_ctas(op, c)
-            results[c] = _time(calls[op], reps)
-        codec.set_launch_ctas(op, 0)
-        results[0] = _time(calls[op], reps)
-        choice = min(results, key=results.get)
-        best[op] = {"ctas_per_sm": int(choice), "ms": results[choice], "sweep_ms": {str(k): v for k, v in results.items()}}
+        for resolver in ((1, 0) if op in ENCODERS else (1,)):
+            if op in ENCODERS:
+                codec.set_resolver(op, bool(resolver))
+            for c in ctas:
+                codec.set_launch_ctas(op, c)
+                results[(c, resolver)] = _time(calls[op], reps)
+        (c, resolver), ms = min(results.items(), key=lambda kv: kv[1])
+        best[op] = {"ctas_per_sm": int(c), "resolver": int(resolver), "ms": ms,
+                    "sweep_ms": {f"{k[0]}/{k[1]}": v for k, v in sorted(results.items())}}
+        set_params(codec, {op: best[op]})
     codec.sync()
     return best
 
 
-def load_cache() -> dict:
+def _load(path) -> dict:
     try:
-        with open(cache_path()) as f:
+        with open(path) as f:
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+def load_cache() -> dict:
+    return _load(cache_path())
 
 
 def save_cache(d: dict) -> None:
@@ -113,14 +152,31 @@ def save_cache(d: dict) -> None:
     os.replace(tmp, p)
 
 
-def apply(codec: Codec, n_bytes: int, tune_on_miss: bool = True) -> dict:
-    """Sets the cached (or freshly tuned) launch shapes for n_bytes inputs."""
-    cache = load_cache()
-    key = _key(codec, n_bytes)
-    if key not in cache and tune_on_miss:
-        cache[key] = tune(codec, n_bytes=min(max(n_bytes, 1 << 20), 256 << 20))
-        save_cache(cache)
-    best = cache.get(key, {})
-    for op, v in best.items():
-        codec.set_launch_ctas(op, v["ctas_per_sm"])
-    return best
+def lookup(device, n_bytes: int):
+    """(params, source) for a device and input size: the user cache, then the
+    table shipped for this GPU, else (None, "defaults")."""
+    k = key(device, n_bytes)
+    c = load_cache()
+    if k in c:
+        return c[k], "cache"
+    shipped = _load(shipped_path(device))
+    sc = size_class(n_bytes)
+    if sc in shipped:
+        return shipped[sc], "shipped"
+    return None, "defaults"
+
+
+def apply(codec: Codec, n_bytes: int | None = None, tune_on_miss: bool = False) -> dict:
+    """Sets the tuned parameters for inputs of n_bytes (default size class
+    when None) on the context and returns {"params", "source"}."""
+    nb = n_bytes if n_bytes is not None else 256 << 20
+    params, source = lookup(codec.device, nb)
+    if params is None and tune_on_miss:
+        params = tune(codec, n_bytes=min(max(nb, 1 << 20), 512 << 20))
+        c = load_cache()
+        c[key(codec.device, nb)] = params
+        save_cache(c)
+        source = "tuned"
+    if params is not None:
+        set_params(codec, params)
+    return {"params": params, "source": source}

@@ -892,7 +892,7 @@ __device__ __forceinline__ void run_helper(Ctl& sm, const Src& src, const Sync& 
   begin_launch(sm, sy);
   __syncthreads();
   const int warp = threadIdx.x >> 5;
-  if (RESOLVE && warp == 0) resolve_loop(sy, sm.epoch, src.total);
+  if (RESOLVE && sy.resolver && warp == 0) resolve_loop(sy, sm.epoch, src.total);
   if (SCAN && warp == 1) src.scan(sm.epoch);
 }
 
@@ -1080,6 +1080,7 @@ struct cortado_ctx {
   unsigned int* words = nullptr;  // [0] queue, [1] finished, [2] status, [3..4] minmax, [5] epoch, [6] helper ticket
   int grid_batch[6] = {0, 0, 0, 0, 0, 0};
   int ctas_override[6] = {0, 0, 0, 0, 0, 0};  // per op: resident CTAs per SM (0 = occupancy limit)
+  int resolver[6] = {1, 1, 1, 1, 1, 1};        // per op: lookback resolver warp on (encoders)
   // Item tables of the batched launch: a ring of ITEM_SLOTS slots, each with
   // items_cap entries in pinned host staging and in device memory, and an
   // event recorded after the launch that read it.  A call waits only for the
@@ -1183,7 +1184,7 @@ cortado_status ensure_items(cortado_ctx* ctx, int n_items) {
   return CORTADO_OK;
 }
 
-Sync next_sync(cortado_ctx* ctx, cudaStream_t) {
+Sync next_sync(cortado_ctx* ctx, cudaStream_t, int op = 0) {
   Sync s;
   s.flags = ctx->flags;
   s.offs = ctx->flags + ctx->flags_cap;
@@ -1192,6 +1193,7 @@ Sync next_sync(cortado_ctx* ctx, cudaStream_t) {
   s.status = ctx->words + 2;
   s.epoch = ctx->words + 5;
   s.timeout_ns = ctx->timeout_ns;
+  s.resolver = ctx->resolver[op];
   return s;
 }
 
@@ -1327,6 +1329,12 @@ cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas
   return CORTADO_OK;
 }
 
+cortado_status cortado_set_resolver(cortado_ctx* ctx, cortado_op op, int enabled) {
+  if (!ctx || op < CORTADO_OP_STORE || op > CORTADO_OP_RESI_RECV) return CORTADO_ERR_INVALID_ARG;
+  ctx->resolver[op] = enabled ? 1 : 0;
+  return CORTADO_OK;
+}
+
 cortado_status cortado_selftest_timeout(cortado_ctx* ctx, cortado_stream_t stream) {
   if (!ctx) return CORTADO_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
@@ -1365,7 +1373,7 @@ cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t 
   a.out_size = (long long*)d_outsize;
   a.n = n_bytes;
   a.q1 = make_quant(e);
-  a.sy = next_sync(ctx, st);
+  a.sy = next_sync(ctx, st, OP_STORE);
   CUtensorMap map;
   a.has_map_in = make_rows_map(&map, d_in, n_bytes);
   k_store<<<grid_for(tuned_grid(ctx, OP_STORE, ctx->grid_store), chunks), NT, SMEM_STD, st>>>(a, map);
@@ -1396,7 +1404,7 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.q1 = make_quant(e1);
   a.q2 = make_quant(e2);
   a.client = (uint8_t*)d_client;
-  a.sy = next_sync(ctx, st);
+  a.sy = next_sync(ctx, st, op);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
   if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
   else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
@@ -1449,7 +1457,7 @@ static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int
   a.out_cap = out_capacity;
   a.out_size = (long long*)d_outsize;
   a.n = n_bytes;
-  a.sy = next_sync(ctx, st);
+  a.sy = next_sync(ctx, st, op);
   CUtensorMap msrc, mout;
   memset(&msrc, 0, sizeof(msrc));
   // The output map needs the decoded size, which only the stream header holds:
@@ -1572,7 +1580,7 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   cudaEventSynchronize(ctx->items_done[slot]);  // the launch that last read this slot has ended
   BatchItem* h_tab = ctx->h_items + (size_t)slot * ctx->items_cap;
   BatchItem* d_tab = ctx->d_items + (size_t)slot * ctx->items_cap;
-  const Sync sy = next_sync(ctx, st);
+  const Sync sy = next_sync(ctx, st, op);
   long long base = 0;
   for (int i = 0; i < n_items; i++) {
     const cortado_item& it = items[i];
@@ -1696,6 +1704,7 @@ cortado_status cortado_store_encode_noalloc(const void* d_in, int64_t n_bytes, f
   a.sy.status = a.sy.counter + 2;
   a.sy.epoch = a.sy.counter + 3;
   a.sy.timeout_ns = 2000000000ull;
+  a.sy.resolver = 1;
   CUtensorMap map;
   a.has_map_in = make_rows_map(&map, d_in, n_bytes);
   k_store_noalloc<<<grid_for(d.grid, chunks_of(n_bytes)), NT, SMEM_STD, st>>>(a, map);

@@ -60,6 +60,7 @@ struct Sync {
   unsigned int* status;       // first error latched
   unsigned int* epoch;        // 0..65535, tags this launch's lookback words
   unsigned long long timeout_ns;
+  int resolver;               // encoders: the helper CTA resolves lookback prefixes ahead of the flushes
 };
 
 // ---------------------------------------------------------------- PTX helpers

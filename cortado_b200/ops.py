@@ -60,7 +60,9 @@ def eb_exponent(eb_abs: float) -> int:
 class Codec:
     """One libcortado context (scratch for one stream at a time) on a device."""
 
-    def __init__(self, device: int | torch.device | None = None):
+    def __init__(self, device: int | torch.device | None = None, tuned: bool = True):
+        """tuned: set the autotuner's launch parameters for this GPU (the user
+        cache, else the table shipped for it; see cortado_b200.autotune)."""
         if not torch.cuda.is_available():
             raise RuntimeError("cortado_b200 needs a CUDA device")
         if device is None:
@@ -71,6 +73,10 @@ class Codec:
         with torch.cuda.device(self.device):
             check(self._L.cortado_create(ctypes.byref(h), self.device.index), "cortado_create")
         self._h = h
+        self.tuning = {"params": None, "source": "defaults"}
+        if tuned:
+            from . import autotune
+            self.tuning = autotune.apply(self)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -100,6 +106,10 @@ class Codec:
     def set_launch_ctas(self, op: str, ctas_per_sm: int):
         """Persistent-grid size of one operation (0 = occupancy limit)."""
         check(self._L.cortado_set_launch_ctas(self._h, _native.OPS[op], int(ctas_per_sm)), "set_launch_ctas")
+
+    def set_resolver(self, op: str, enabled: bool):
+        """Lookback resolver warp of an encoder's launches on or off."""
+        check(self._L.cortado_set_resolver(self._h, _native.OPS[op], int(bool(enabled))), "set_resolver")
 
     def sync(self, stream=None):
         """Waits for the stream and raises the first device-detected error."""

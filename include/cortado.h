@@ -203,6 +203,14 @@ cortado_status cortado_reserve(cortado_ctx* ctx, int64_t chunks, int items);
  * it changes speed only, never output bytes. */
 cortado_status cortado_set_launch_ctas(cortado_ctx* ctx, cortado_op op, int ctas_per_sm);
 
+/* Whether launches of `op` on this context give a warp of their helper CTA
+ * to resolving lookback prefixes ahead of the flushes (encoders; default 1).
+ * With 0, each chunk's flush walks the lookback words itself.  Chosen by the
+ * autotuner (cortado_b200/autotune.py); it changes speed only, never output
+ * bytes.  No counterpart in the reference (its lookback is a per-chunk spin,
+ * include/d_compression.h:120-160). */
+cortado_status cortado_set_resolver(cortado_ctx* ctx, cortado_op op, int enabled);
+
 /* store without allocating: for callers that cannot call cudaMalloc.
  *
  * No counterpart in the reference.  Some callers of this library cannot
