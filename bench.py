@@ -13,7 +13,11 @@ reference's throughput convention, insize * 1e-9 / runtime, applied to the
 whole flow; per-operation rates are reported under "ops").  Inputs are larger
 than the 126 MB L2, so no flush is needed between steps.
 
-``value`` is timed with CUDA events with the field resident in HBM.  ``e2e``
+``value`` is timed with CUDA events with the field resident in HBM; the
+range stays in device memory and the kernels scale the NOA bounds, so the
+steps are enqueued back to back (``value_host_scaled``: the same flow with
+the range handed to the host for the scaling, as the reference's drivers
+do).  ``e2e``
 times the same flow through the C ABI with host buffers: every step copies
 the field from pinned host memory to the device and copies the two streams
 sent to the client and the final reconstruction back.
@@ -118,11 +122,19 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- GPU arm
 class Flow:
-    """Preallocated buffers and the six calls of one step on one stream."""
+    """Preallocated buffers and the six calls of one step on one stream.
 
-    def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream, abs_mode: bool = False):
+    device_noa: the range stays in device memory and the NOA entry points
+    scale the bounds in the kernels, so nothing in a step waits for the host
+    (the same streams as the host-scaled calls); False: the range is handed
+    to the host, which scales the bounds, as the reference's drivers do."""
+
+    def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream, abs_mode: bool = False,
+                 device_noa: bool = True):
         from cortado_b200 import ops
         self.c, self.x, self.s, self.abs_mode = codec, x, stream, abs_mode
+        self.device_noa = device_noa
+        self.mm = torch.empty(2, dtype=torch.float32, device=x.device)
         self.stream = stream  # the compute stream, as cortado_b200.pipeline expects
         dev = x.device
         self.n = x.numel() * 4
@@ -145,6 +157,8 @@ class Flow:
                 float(storage.noa_scale(EB_DST, rng)))
 
     def step(self, timed=False):
+        if self.device_noa:
+            return self.step_device_noa(timed)
         c, s, sz = self.c, self.s, self.sizes
         if timed:
             self.ev[0].record(s)
@@ -166,6 +180,36 @@ class Flow:
         c.residual_apply(self.cl, self.n, self.resi, self.fin, sz[4:5], stream=s)
         if timed:
             self.ev[6].record(s)
+
+    def step_device_noa(self, timed=False):
+        from cortado_b200 import storage
+        c, s, sz, mm = self.c, self.s, self.sizes, self.mm
+        ev = self.ev if timed else [None] * len(self.ev)
+        rec = (lambda i: ev[i].record(s)) if timed else (lambda i: None)
+        rec(0)
+        c.INOA_find_range_device(self.x, mm, stream=s)  # computed in both modes, as the reference's store does
+        rec(1)
+        if self.abs_mode:
+            a, b, d = (float(storage.f32(e)) for e in (ABS_STORE, ABS_SRC, ABS_DST))
+            c.server_encode(self.x, self.n, self.stor, sz[0:1], a, stream=s)
+            rec(2)
+            c.s2c_encode(self.stor, self.init, sz[1:2], b, self.n, stream=s)
+            rec(3)
+            c.client_decode(self.init, self.cl, sz[2:3], stream=s)
+            rec(4)
+            c.residual_encode(self.stor, self.resi, sz[3:4], b, d, self.n, stream=s)
+        else:
+            a, b, d = (float(storage.f32(e)) for e in (EB_STORE, EB_SRC, EB_DST))
+            c.server_encode_noa(self.x, self.n, self.stor, sz[0:1], mm, a, stream=s)
+            rec(2)
+            c.s2c_encode_noa(self.stor, self.init, sz[1:2], mm, b, self.n, stream=s)
+            rec(3)
+            c.client_decode(self.init, self.cl, sz[2:3], stream=s)
+            rec(4)
+            c.residual_encode_noa(self.stor, self.resi, sz[3:4], mm, b, d, self.n, stream=s)
+        rec(5)
+        c.residual_apply(self.cl, self.n, self.resi, self.fin, sz[4:5], stream=s)
+        rec(6)
 
     def op_ms(self):
         return [self.ev[i].elapsed_time(self.ev[i + 1]) for i in range(len(OPS))]
@@ -207,21 +251,36 @@ def _run_gpu(args, rank, world):
         sizes = fl.sizes.cpu().tolist()
     barrier(world)
     torch.cuda.synchronize(dev)
-    per_op = np.zeros(len(OPS))
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        start.record(stream)
-        for _ in range(args.steps):
-            fl.step(timed=True)
-            stream.synchronize()
-            per_op += np.array(fl.op_ms())
-        end.record(stream)
-        torch.cuda.synchronize(dev)
-    ms = start.elapsed_time(end)
+    def timed_steps(flow, k):
+        """k steps enqueued back to back (the device-NOA flow waits for nothing
+        on the host), each with its own events; returns (ms per step, mean ms
+        per operation)."""
+        sets = [[torch.cuda.Event(enable_timing=True) for _ in range(len(OPS) + 1)] for _ in range(k)]
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(flow.s):
+            st.record(flow.s)
+            for evs in sets:
+                flow.ev = evs
+                flow.step(timed=True)
+            en.record(flow.s)
+            torch.cuda.synchronize(dev)
+        ops = np.mean([[e[i].elapsed_time(e[i + 1]) for i in range(len(OPS))] for e in sets], axis=0)
+        return st.elapsed_time(en) / k, ops
+
+    ms, per_op = timed_steps(fl, args.steps)
     codec.sync(stream)
-    ms = max_over_ranks(ms, world, dev)
-    per_op /= args.steps
+    ms = max_over_ranks(ms * args.steps, world, dev)
     n = fl.n
+    # the same flow with the range handed to the host, which scales the bounds
+    # (the reference drivers' way; every step waits for the device once)
+    fh = Flow(codec, x, stream, device_noa=False)
+    with torch.cuda.stream(stream):
+        fh.step()
+        codec.sync(stream)
+    ms_host, per_op_host = timed_steps(fh, args.steps)
+    codec.sync(stream)
+    ms_host = max_over_ranks(ms_host, world, dev)
+    del fh
 
     # Reference-style timing of each operation: the host clock around one call
     # and a stream synchronize, median of 10 after a warm-up, as the
@@ -305,19 +364,12 @@ def _run_gpu(args, rank, world):
         abs_ok = bool(torch.all((fa.fin - x).abs() <= eb_a))
         abs_sizes = fa.sizes.cpu().tolist()
         a_steps = max(1, min(args.steps, 5))
-        a_op = np.zeros(len(OPS))
         barrier(world)
         torch.cuda.synchronize(dev)
-        start.record(stream)
-        for _ in range(a_steps):
-            fa.step(timed=True)
-            stream.synchronize()
-            a_op += np.array(fa.op_ms())
-        end.record(stream)
-        torch.cuda.synchronize(dev)
-    abs_ms = max_over_ranks(start.elapsed_time(end) / a_steps, world, dev)
+    abs_ms, a_op = timed_steps(fa, a_steps)
+    abs_ms = max_over_ranks(abs_ms, world, dev)
     codec.sync(stream)
-    abs_res = dict(ms=abs_ms, per_op=a_op / a_steps, sizes=abs_sizes, ok=abs_ok)
+    abs_res = dict(ms=abs_ms, per_op=a_op, sizes=abs_sizes, ok=abs_ok)
     x_host = x.cpu().numpy()
     # The reference's own CUDA build on the same field, bounds and GPU, in the
     # same clock-sampled window (a reported baseline; one GPU only).
@@ -325,6 +377,7 @@ def _run_gpu(args, rank, world):
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = reference_cuda_baseline(x_host)
     return dict(abs=abs_res, ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
+                ms_host=ms_host, per_op_host=per_op_host,
                 h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda, tuning=tuning)
 
 
@@ -668,6 +721,9 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "per_kernel_frac": {k: alg[k] / (op_ms[k] * 1e-3) * 1e-9 / peak for k in alg}},
+        # the same flow with the range handed to the host for the bounds' scaling
+        "value_host_scaled": {"value": job_gbs(n, world, r["ms_host"]), "ms_per_step": r["ms_host"],
+                              "ops_ms": dict(zip(OPS, [float(v) for v in r["per_op_host"]]))},
         "e2e": {"value": world * n * 1e-9 / (r["e2e_ms"] * 1e-3), "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
         # one kernel per operation, two for the NOA range (min/max, hand-over)

@@ -42,6 +42,10 @@ SIGNATURES = {
     "cortado_reserve": (_int, [_vp, _i64, _int]),
     "cortado_selftest_timeout": (_int, [_vp, _vp]),
     "cortado_init_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _vp, _i64, _vp, _vp, _vp]),
+    "cortado_noa_range_device": (_int, [_vp, _vp, _i64, _vp, _vp]),
+    "cortado_store_encode_noa": (_int, [_vp, _vp, _i64, _vp, _f32, _vp, _i64, _vp, _vp]),
+    "cortado_init_send_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _vp, _i64, _vp, _vp]),
+    "cortado_resi_send_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _f32, _vp, _i64, _vp, _vp]),
     "cortado_resi_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _f32, _vp, _i64, _vp, _vp, _vp]),
 }
 

@@ -134,6 +134,11 @@ struct SingleSrc {
   const CUtensorMap* map_out;
   long long total;
   StreamHdr h;
+  Quant q1, q2;  // the bounds' quantizers (resolved on the device for NOA entry points)
+  __device__ __forceinline__ void quant(int, Quant& x1, Quant& x2) const {
+    x1 = q1;
+    x2 = q2;
+  }
   __device__ __forceinline__ int locate(long long g, int, long long& c) const {
     c = g;
     return 0;
@@ -184,6 +189,10 @@ struct BatchSrc {
     }
   }
   __device__ __forceinline__ const OpArgs& args(int i) const { return items[i].a; }
+  __device__ __forceinline__ void quant(int i, Quant& x1, Quant& x2) const {
+    x1 = items[i].a.q1;
+    x2 = items[i].a.q2;
+  }
   __device__ __forceinline__ const CUtensorMap* min(int i) const { return &items[i].map_in; }
   __device__ __forceinline__ const CUtensorMap* mout(int i) const { return &items[i].map_out; }
   __device__ __forceinline__ StreamHdr header(int i) const { return read_header(items[i].a.in, items[i].a.in_bytes); }
@@ -462,10 +471,11 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
       load_plain_rows(A, A_.in, c, nw);
       __syncthreads();
     }
-    if (Src::batched && c == 0 && tid == 0) write_header(A_.out, A_.n, A_.q1.eb_e);
+    Quant q1, q2_unused;
+    src.quant(item, q1, q2_unused);
+    if (Src::batched && c == 0 && tid == 0) write_header(A_.out, A_.n, q1.eb_e);
     uint32_t v[32];
     row_load(A, tid, v);
-    const Quant q1 = A_.q1;
     {
       // the float form; a warp that holds lossless words (inf, NaN included)
       // chooses per word
@@ -635,7 +645,8 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       // stored bins -> floats (iSQ, skipped for chunks stored as floats) ->
       // request bins (CQ, d_s2c.h:132-137) or residuals (d_RESI_4.h:57-76)
       const Quant qs = make_quant(m.eb_e);
-      const Quant q1 = A.q1, q2 = A.q2;
+      Quant q1, q2;
+      src.quant(item, q1, q2);
       // Shift form, when every word of the warp allows it: a lossy stored bin
       // a (|a| < 2^23) is the float a * 2^(e_s - 126), so its request bin is
       // a / 2^k1 rounded half away from zero (k1 = e_1 - e_s >= 0), and the
@@ -899,12 +910,18 @@ __device__ __forceinline__ void run_helper(Ctl& sm, const Src& src, const Sync& 
 // ---- single-stream kernels
 __global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant__ OpArgs a, const __grid_constant__ CUtensorMap map_in) {
   Ctl& sm = ctl_block();
-  const long long chunks = (a.n + CS - 1) / CS;
+  Quant q1, q2;
+  const unsigned int noa_err = resolve_noa(a, q1, q2);  // every thread, the same result
+  const long long chunks = noa_err ? 0 : (a.n + CS - 1) / CS;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    write_header(a.out, a.n, a.q1.eb_e);
-    if (chunks == 0) *a.out_size = HDR;
+    if (noa_err) {
+      latch(a.sy.status, noa_err);  // nothing is written, as the host path writes nothing
+    } else {
+      write_header(a.out, a.n, q1.eb_e);
+      if (chunks == 0) *a.out_size = HDR;
+    }
   }
-  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
+  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}, q1, q2};
   if (helper_cta(sm, a.sy)) run_helper<true, false>(sm, src, a.sy);
   else store_loop(sm, src, a.sy);
   finish_launch(sm, a.sy);
@@ -916,12 +933,19 @@ __global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_consta
   StreamHdr h = read_header(a.in, a.in_bytes);
   const bool hdr_ok = h.ok && h.n == a.n;
   if (!hdr_ok) h.chunks = 0;
+  Quant q1, q2;
+  const unsigned int noa_err = resolve_noa(a, q1, q2);  // every thread, the same result
+  if (noa_err) h.chunks = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
-    write_header(a.out, hdr_ok ? h.n : 0, (OP == OP_S2C) ? a.q1.eb_e : a.q2.eb_e);
-    if (h.chunks == 0) *a.out_size = HDR;
+    if (noa_err) {
+      latch(a.sy.status, noa_err);  // nothing is written, as the host path writes nothing
+    } else {
+      if (!hdr_ok) latch(a.sy.status, h.ok ? DST_SIZE_MISMATCH : DST_CORRUPT);
+      write_header(a.out, hdr_ok ? h.n : 0, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
+      if (h.chunks == 0) *a.out_size = HDR;
+    }
   }
-  const SingleSrc src{&a, nullptr, nullptr, h.chunks, h};
+  const SingleSrc src{&a, nullptr, nullptr, h.chunks, h, q1, q2};
   if (helper_cta(sm, a.sy)) run_helper<true, true>(sm, src, a.sy);
   else reencode_loop<OP>(sm, src, a.sy);
   finish_launch(sm, a.sy);
@@ -939,7 +963,7 @@ __global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) 
     if (!hdr_ok) latch(a.sy.status, !h.ok ? DST_CORRUPT : (OP == OP_RAPPLY && h.n != a.n) ? DST_SIZE_MISMATCH : DST_CAPACITY);
     *a.out_size = hdr_ok ? h.n : 0;
   }
-  const SingleSrc src{&a, &map_src, &map_out, h.chunks, h};
+  const SingleSrc src{&a, &map_src, &map_out, h.chunks, h, a.q1, a.q2};
   if (helper_cta(sm, a.sy)) run_helper<false, true>(sm, src, a.sy);
   else decode_loop<OP>(sm, src, a.sy);
   finish_launch(sm, a.sy);
@@ -979,7 +1003,7 @@ __global__ void __launch_bounds__(NT, MINB_STORE) k_store_noalloc(const __grid_c
     write_header(a.out, a.n, a.q1.eb_e);
     if (chunks == 0) *a.out_size = HDR;
   }
-  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}};
+  const SingleSrc src{&a, &map_in, nullptr, chunks, StreamHdr{}, a.q1, a.q2};
   if (helper_cta(sm, a.sy)) run_helper<true, false>(sm, src, a.sy);
   else store_loop(sm, src, a.sy);
   const unsigned int st = finish_launch(sm, a.sy, true);
@@ -1058,6 +1082,16 @@ __global__ void k_range_publish(unsigned int* words, volatile unsigned int* host
   words[0] = 0xffffffffu;
   words[1] = 0u;
   __threadfence_system();
+}
+
+// The range for the device-side NOA entry points: min and max as floats into
+// device memory (no host hand-over), and the reduction words reset.
+__global__ void k_range_to_device(unsigned int* words, float* out) {
+  auto unord = [](unsigned int o) { return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o); };
+  out[0] = unord(words[0]);
+  out[1] = unord(words[1]);
+  words[0] = 0xffffffffu;
+  words[1] = 0u;
 }
 
 // Failure-detection self-test: one thread waits, through the decoders' own
@@ -1382,19 +1416,27 @@ cortado_status cortado_store_encode(cortado_ctx* ctx, const void* d_in, int64_t 
 
 static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
                                float eb1, float eb2, void* d_out, int64_t out_capacity, int64_t* d_outsize,
-                               cortado_stream_t stream, void* d_client = nullptr) {
+                               cortado_stream_t stream, void* d_client = nullptr, const float* d_minmax = nullptr) {
   if (!ctx || !d_stored || !d_out || !d_outsize || n_bytes < 0 || (n_bytes & 3) || stored_bytes < HDR)
     return CORTADO_ERR_INVALID_ARG;
   if (!aligned16(d_stored) || !aligned16(d_out) || (d_client && !aligned16(d_client))) return CORTADO_ERR_ALIGNMENT;
   if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
-  int e1 = 0, e2 = 0;
-  cortado_status s = eb_exponent(eb1, &e1);
-  if (s) return s;
-  if (op == OP_RESI && (s = eb_exponent(eb2, &e2))) return s;
+  int e1 = 1, e2 = 1;
+  cortado_status s = CORTADO_OK;
+  if (!d_minmax) {  // NOA bounds are checked on the device
+    if ((s = eb_exponent(eb1, &e1))) return s;
+    if (op == OP_RESI && (s = eb_exponent(eb2, &e2))) return s;
+  }
   const int64_t chunks = chunks_of(n_bytes);
   cudaStream_t st = (cudaStream_t)stream;
   if ((s = ensure_flags(ctx, chunks, st))) return s;
   OpArgs a{};
+  if (d_minmax) {
+    a.noa = d_minmax;
+    a.noa_eb1 = eb1;
+    a.noa_eb2 = eb2;
+    a.noa_mode = (op == OP_S2C) ? 2 : 3;
+  }
   a.in = (const uint8_t*)d_stored;
   a.in_bytes = stored_bytes;
   a.out = (uint8_t*)d_out;
@@ -1438,6 +1480,64 @@ cortado_status cortado_resi_send_apply(cortado_ctx* ctx, const void* d_stored, i
   if (!d_client && n_bytes) return CORTADO_ERR_INVALID_ARG;
   return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_abs, dst_eb_abs, d_out, out_capacity, d_outsize,
                   stream, d_client);
+}
+
+cortado_status cortado_noa_range_device(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* d_minmax,
+                                        cortado_stream_t stream) {
+  if (!ctx || !d_in || !d_minmax || n_bytes <= 0 || (n_bytes & 3)) return CORTADO_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long nw = n_bytes / 4;
+  long long blocks = (nw / 4 + 1023) / 1024;
+  if (blocks > 8L * ctx->sms) blocks = 8L * ctx->sms;
+  if (blocks < 1) blocks = 1;
+  k_minmax<<<(int)blocks, 256, 0, st>>>((const float*)d_in, nw, ctx->words + 3);
+  k_range_to_device<<<1, 1, 0, st>>>(ctx->words + 3, d_minmax);
+  return launch_status(cudaSuccess);
+}
+
+cortado_status cortado_store_encode_noa(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, const float* d_minmax,
+                                        float eb_noa, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                        cortado_stream_t stream) {
+  if (!ctx || (!d_in && n_bytes) || !d_out || !d_outsize || !d_minmax || n_bytes < 0 || (n_bytes & 3))
+    return CORTADO_ERR_INVALID_ARG;
+  if (!aligned16(d_in) || !aligned16(d_out)) return CORTADO_ERR_ALIGNMENT;
+  if (out_capacity < cortado_max_stream_bytes(n_bytes)) return CORTADO_ERR_CAPACITY;
+  const int64_t chunks = chunks_of(n_bytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  cortado_status s = ensure_flags(ctx, chunks, st);
+  if (s) return s;
+  OpArgs a{};
+  a.in = (const uint8_t*)d_in;
+  a.in_bytes = n_bytes;
+  a.out = (uint8_t*)d_out;
+  a.out_cap = out_capacity;
+  a.out_size = (long long*)d_outsize;
+  a.n = n_bytes;
+  a.q1 = make_quant(1);
+  a.noa = d_minmax;
+  a.noa_eb1 = eb_noa;
+  a.noa_mode = 1;
+  a.sy = next_sync(ctx, st, OP_STORE);
+  CUtensorMap map;
+  a.has_map_in = make_rows_map(&map, d_in, n_bytes);
+  k_store<<<grid_for(tuned_grid(ctx, OP_STORE, ctx->grid_store), chunks), NT, SMEM_STD, st>>>(a, map);
+  return launch_status(cudaSuccess);
+}
+
+cortado_status cortado_init_send_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                     const float* d_minmax, float request_eb_noa, void* d_out, int64_t out_capacity,
+                                     int64_t* d_outsize, cortado_stream_t stream) {
+  if (!d_minmax) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_S2C, d_stored, stored_bytes, n_bytes, request_eb_noa, 0.0f, d_out, out_capacity, d_outsize,
+                  stream, nullptr, d_minmax);
+}
+
+cortado_status cortado_resi_send_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                     const float* d_minmax, float src_eb_noa, float dst_eb_noa, void* d_out,
+                                     int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream) {
+  if (!d_minmax) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_noa, dst_eb_noa, d_out, out_capacity,
+                  d_outsize, stream, nullptr, d_minmax);
 }
 
 static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int64_t stream_bytes, const void* d_src,

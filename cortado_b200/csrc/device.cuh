@@ -28,6 +28,8 @@ constexpr int HDR = 16;     // stream header bytes
 // Device-latched status codes (same values as cortado_status).
 enum : uint32_t {
   DST_OK = 0,
+  DST_EB_TOO_SMALL = 1,
+  DST_EB_TOO_LARGE = 2,
   DST_CORRUPT = 3,
   DST_SIZE_MISMATCH = 4,
   DST_TIMEOUT = 5,

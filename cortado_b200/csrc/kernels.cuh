@@ -31,7 +31,40 @@ struct OpArgs {
   Sync sy;
   int has_map_in, has_map_out;
   uint8_t* client;          // init_send / resi_send with apply: the client's reconstruction (floats), or null
+  // NOA bounds resolved on the device (cortado_*_noa): q1/q2 come from
+  // noa_eb1/noa_eb2 times the range max - min of noa[0..1] (device floats)
+  const float* noa;
+  float noa_eb1, noa_eb2;
+  int noa_mode;             // 0: q1/q2 as given; 1: store (half of eb1); 2: init (eb1); 3: residual (eb1, eb2)
 };
+
+// The NOA bounds of the drivers (src/cortado_store.cu:222-227,
+// src/cortado_init.cu:294-296, src/cortado_resi.cu:329-332), evaluated on the
+// device: eb_abs = float(max - min) * eb, each step rounded once, the store's
+// bins at eb_abs / 2, then the checks and biased exponent of the host-side
+// eb_exponent.  Returns 0 or the status to latch.
+__device__ __forceinline__ unsigned int noa_exponent(float eb, int* e) {
+  if (!(eb >= 1.17549435e-38f)) return (eb != eb) ? DST_EB_TOO_LARGE : DST_EB_TOO_SMALL;  // FLT_MIN
+  const int be = (int)((__float_as_uint(eb) >> 23) & 0xffu);
+  if (be + 24 >= 255) return DST_EB_TOO_LARGE;
+  *e = be;
+  return 0;
+}
+__device__ __forceinline__ unsigned int resolve_noa(const OpArgs& a, Quant& q1, Quant& q2) {
+  q1 = a.q1;
+  q2 = a.q2;
+  if (!a.noa_mode) return 0;
+  const float range = __fsub_rn(a.noa[1], a.noa[0]);
+  float eb1 = __fmul_rn(range, a.noa_eb1);
+  if (a.noa_mode == 1) eb1 = __fdiv_rn(eb1, 2.0f);  // stored bins use half the bound
+  int e1 = 1, e2 = 1;
+  unsigned int st = noa_exponent(eb1, &e1);
+  if (!st && a.noa_mode == 3) st = noa_exponent(__fmul_rn(range, a.noa_eb2), &e2);
+  if (st) return st;
+  q1 = make_quant(e1);
+  if (a.noa_mode == 3) q2 = make_quant(e2);
+  return 0;
+}
 
 // ---------------------------------------------------------------- shared memory
 // A CTA owns a 1 KiB control block followed by two chunk buffers of

@@ -173,6 +173,37 @@ class Codec:
                                         _stream(stream)), "INOA_find_range")
         return lo.value, hi.value
 
+    # ------------------------------------------------ NOA bounds on the device
+    def INOA_find_range_device(self, d_data, d_minmax=None, size=None, stream=None):
+        """The range into a device float32 tensor [min, max] without waiting
+        for the device (the NOA entry points below read it there)."""
+        if d_minmax is None:
+            d_minmax = torch.empty(2, dtype=torch.float32, device=self.device)
+        n = _nbytes(d_data) if size is None else int(size)
+        check(self._L.cortado_noa_range_device(self._h, _ptr(d_data), n, _ptr(d_minmax), _stream(stream)),
+              "INOA_find_range_device")
+        return d_minmax
+
+    def server_encode_noa(self, d_input, insize, d_output, d_outsize, d_minmax, eb_noa, stream=None):
+        check(self._L.cortado_store_encode_noa(self._h, _ptr(d_input), int(insize), _ptr(d_minmax), float(eb_noa),
+                                               _ptr(d_output), _nbytes(d_output), _ptr(d_outsize), _stream(stream)),
+              "server_encode_noa")
+
+    def s2c_encode_noa(self, d_input, d_output, d_outsize, d_minmax, request_eb_noa, n_bytes, in_bytes=None,
+                       stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_init_send_noa(self._h, _ptr(d_input), n, int(n_bytes), _ptr(d_minmax),
+                                            float(request_eb_noa), _ptr(d_output), _nbytes(d_output),
+                                            _ptr(d_outsize), _stream(stream)), "s2c_encode_noa")
+
+    def residual_encode_noa(self, d_input, d_output, d_outsize, d_minmax, src_eb_noa, dest_eb_noa, n_bytes,
+                            in_bytes=None, stream=None):
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_resi_send_noa(self._h, _ptr(d_input), n, int(n_bytes), _ptr(d_minmax),
+                                            float(src_eb_noa), float(dest_eb_noa), _ptr(d_output),
+                                            _nbytes(d_output), _ptr(d_outsize), _stream(stream)),
+              "residual_encode_noa")
+
     def verify_bound(self, orig, recon, eb_abs, first_bad=None, stream=None):
         """MAXABS_f32 on the device: returns the int64 tensor holding the first
         violating index (or -1 when every value is within eb_abs)."""

@@ -138,6 +138,35 @@ cortado_status cortado_resi_send_apply(cortado_ctx* ctx, const void* d_stored, i
 cortado_status cortado_noa_range(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* h_min, float* h_max,
                                  cortado_stream_t stream);
 
+/* ---- NOA bounds on the device: nothing waits for the host ----
+ * The reference's drivers scale a normalized (NOA) bound on the host,
+ * eb_abs = (max - min) * eb, after copying the range to the host
+ * (src/cortado_store.cu:206-227, include/preprocessors/include/INOA_f32.h:52-61),
+ * so every NOA operation waits for the device.  These entry points keep the
+ * range in device memory and scale the bounds in the kernels with the same
+ * float arithmetic (one rounding for the difference, one for the product,
+ * the store's bins at eb_abs / 2): streams are byte-identical to the
+ * host-scaled calls with storage.noa_scale's bounds.  A whole NOA flow can
+ * then be enqueued without waiting, or captured in a CUDA graph.  Bound
+ * errors (EB_TOO_SMALL, EB_TOO_LARGE) are latched in the context and
+ * returned by cortado_sync(); such a call writes nothing. */
+/* Range of n_bytes of floats into d_minmax[0] (min) and d_minmax[1] (max),
+ * device floats, NaNs ignored; asynchronous. */
+cortado_status cortado_noa_range_device(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, float* d_minmax,
+                                        cortado_stream_t stream);
+/* store at the NOA bound eb_noa of the range in d_minmax. */
+cortado_status cortado_store_encode_noa(cortado_ctx* ctx, const void* d_in, int64_t n_bytes, const float* d_minmax,
+                                        float eb_noa, void* d_out, int64_t out_capacity, int64_t* d_outsize,
+                                        cortado_stream_t stream);
+/* init_send at the NOA request bound request_eb_noa. */
+cortado_status cortado_init_send_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                     const float* d_minmax, float request_eb_noa, void* d_out, int64_t out_capacity,
+                                     int64_t* d_outsize, cortado_stream_t stream);
+/* resi_send between the NOA bounds src_eb_noa and dst_eb_noa. */
+cortado_status cortado_resi_send_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                     const float* d_minmax, float src_eb_noa, float dst_eb_noa, void* d_out,
+                                     int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream);
+
 /* Bound verifier: writes to *d_first_bad (device) the first index i at which
  * recon[i] violates |orig[i] - recon[i]| <= eb_abs under the reference's
  * MAXABS_f32 rules (include/verifiers/MAXABS_f32.h:40-72; NaN and Inf must
