@@ -52,9 +52,9 @@ ABS_STORE, ABS_SRC, ABS_DST = "1e-6", "1e-3", "1e-5"
 OPS = ("noa_range", "store", "init_send", "init_recv", "resi_send", "resi_recv")
 
 
-def make_field(seed: int, device, shape=SHAPE) -> torch.Tensor:
+def make_field(seed: int, device, shape=SHAPE, outliers: bool = True) -> torch.Tensor:
     from cortado_b200 import fields
-    return fields.sinusoid(shape, seed, outlier_frac=1e-3, device=device).reshape(-1)
+    return fields.sinusoid(shape, seed, outlier_frac=1e-3 if outliers else 0.0, device=device).reshape(-1)
 
 
 def peaks():
@@ -269,7 +269,7 @@ def _run_gpu(args, rank, world):
 
     ms, per_op = timed_steps(fl, args.steps)
     codec.sync(stream)
-    ms = max_over_ranks(ms * args.steps, world, dev)
+    ms = max_over_ranks(ms, world, dev)
     n = fl.n
     # the same flow with the range handed to the host, which scales the bounds
     # (the reference drivers' way; every step waits for the device once)
@@ -343,6 +343,7 @@ def _run_gpu(args, rank, world):
     pipe.sync()
     barrier(world)
     torch.cuda.synchronize(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(pipe.s_in)
     pipe(e_steps)
     end.record(pipe.s_out)
@@ -370,13 +371,36 @@ def _run_gpu(args, rank, world):
     abs_ms = max_over_ranks(abs_ms, world, dev)
     codec.sync(stream)
     abs_res = dict(ms=abs_ms, per_op=a_op, sizes=abs_sizes, ok=abs_ok)
+    del fa
+
+    # The NOA flow on the same generator without the outliers (sinusoids and
+    # noise only, as in the small-field configuration) at this shape: the NOA
+    # range is the signal's own, so the streams are dense.
+    xd = make_field(2 + rank, dev, args.shape, outliers=False)
+    torch.cuda.synchronize(dev)  # generated on the default stream; the flow runs on its own
+    fd = Flow(codec, xd, stream)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            fd.step()
+        codec.sync(stream)
+        _, _, eb_d = fd.bounds()
+        dense_ok = bool(torch.all((fd.fin - xd).abs() <= eb_d))
+        dense_sizes = fd.sizes.cpu().tolist()
+        barrier(world)
+        torch.cuda.synchronize(dev)
+    dense_ms, d_op = timed_steps(fd, a_steps)
+    dense_ms = max_over_ranks(dense_ms, world, dev)
+    codec.sync(stream)
+    dense_res = dict(ms=dense_ms, per_op=d_op, sizes=dense_sizes, ok=dense_ok)
+    del fd, xd
     x_host = x.cpu().numpy()
     # The reference's own CUDA build on the same field, bounds and GPU, in the
     # same clock-sampled window (a reported baseline; one GPU only).
     ref_cuda = None
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = reference_cuda_baseline(x_host)
-    return dict(abs=abs_res, ms=ms / args.steps, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
+    return dict(abs=abs_res, dense=dense_res, sms=torch.cuda.get_device_properties(dev).multi_processor_count,
+                ms=ms, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
                 ms_host=ms_host, per_op_host=per_op_host,
                 h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda, tuning=tuning)
 
@@ -550,12 +574,40 @@ def bench_chain(codec, dev, side=16384, seed=4, reps=5):
     return res
 
 
-def load_traffic():
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+def load_profile(name):
+    p = os.path.join(ROOT, "profiles", name)
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
     return {}
+
+
+def load_traffic():
+    return load_profile("traffic.json")
+
+
+def kernel_fracs(n, sizes, per_op, peak):
+    """Algorithmic HBM bytes of each kernel's launch (its input read once,
+    its output written once), its duration, and their rate as a fraction of
+    the copy peak."""
+    s_stor, s_init, s_resi = sizes[0], sizes[1], sizes[3]
+    alg = {"store": n + s_stor, "init_send": s_stor + s_init, "init_recv": s_init + n,
+           "resi_send": s_stor + s_resi, "resi_recv": 2 * n + s_resi}
+    op_ms = dict(zip(OPS, [float(v) for v in per_op]))
+    return alg, op_ms, {k: alg[k] / (op_ms[k] * 1e-3) * 1e-9 / peak for k in alg}
+
+
+def issue_fracs(n, op_ms, sms, sm_mhz):
+    """The re-encoders move only compressed bytes, so their bound is the
+    instruction issue rate: warp instructions per chunk (from the ncu capture
+    of the NOA flow in profiles/issue.json) x chunks, over 4 issues per SM per
+    cycle at the sampled median SM clock, divided by the measured time."""
+    ipc = load_profile("issue.json").get("inst_per_chunk", {})
+    if not sm_mhz:
+        return None
+    chunks = (n + 16383) // 16384
+    return {k: ipc[k] * chunks / (sms * 4 * sm_mhz * 1e6) / (op_ms[k] * 1e-3)
+            for k in ("init_send", "resi_send") if k in ipc}
 
 
 def host_field(shape, seed=2, sample_mb=0) -> np.ndarray:
@@ -662,8 +714,12 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the shipped launch parameters (no tuning run)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="512,512,512", help="field shape (profiling uses a smaller one)")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched, serving and chain measurements")
+    ap.add_argument("--extras", default="batched,serving,chain", help="which of those to run (comma list)")
+    ap.add_argument("--batched-fields", type=int, default=64, help="fields of the batched measurement")
+    ap.add_argument("--batched-max-mb", type=int, default=256, help="largest field of the batched measurement")
     args = ap.parse_args()
+    extras = set() if args.no_extras else {e for e in args.extras.split(",") if e}
     args.shape = tuple(int(v) for v in args.shape.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -701,12 +757,11 @@ def main():
     ops_gbs = {op: (n * 1e-9 / (t * 1e-3) if t > 0 else None) for op, t in zip(OPS, r["per_op"])}
     sizes = r["sizes"]
     s_stor, s_init, s_resi = sizes[0], sizes[1], sizes[3]
-    # algorithmic HBM bytes per launch of each kernel
-    alg = {"store": n + s_stor, "init_send": s_stor + s_init, "init_recv": s_init + n,
-           "resi_send": s_stor + s_resi, "resi_recv": 2 * n + s_resi}
-    op_ms = dict(zip(OPS, r["per_op"]))
-    dom = max(alg, key=lambda k: op_ms[k])
     peak, peak_kind = peaks()
+    alg, op_ms, fracs = kernel_fracs(n, sizes, r["per_op"], peak)
+    _, abs_ms, abs_fracs = kernel_fracs(n, r["abs"]["sizes"], r["abs"]["per_op"], peak)
+    _, dense_ms, dense_fracs = kernel_fracs(n, r["dense"]["sizes"], r["dense"]["per_op"], peak)
+    dom = max(alg, key=lambda k: op_ms[k])
     achieved = alg[dom] / (op_ms[dom] * 1e-3) * 1e-9
     traffic = load_traffic().get(dom)
     line = {
@@ -720,7 +775,11 @@ def main():
         "bounds_verified": r["ok"],
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                     "per_kernel_frac": {k: alg[k] / (op_ms[k] * 1e-3) * 1e-9 / peak for k in alg}},
+                     "per_kernel_frac": fracs,
+                     "per_kernel_frac_abs": abs_fracs,
+                     "per_kernel_frac_no_outliers": dense_fracs,
+                     # the re-encoders' own bound: the fraction of the SMs' issue rate
+                     "issue_frac": issue_fracs(n, op_ms, r["sms"], r["clocks"].get("sm_mhz"))},
         # the same flow with the range handed to the host for the bounds' scaling
         "value_host_scaled": {"value": job_gbs(n, world, r["ms_host"]), "ms_per_step": r["ms_host"],
                               "ops_ms": dict(zip(OPS, [float(v) for v in r["per_op_host"]]))},
@@ -734,7 +793,15 @@ def main():
                      "stream_bytes": {"stor": r["abs"]["sizes"][0], "init": r["abs"]["sizes"][1],
                                       "resi": r["abs"]["sizes"][3]},
                      "ops": {k: {"ms": t, "orig_GBps": n * 1e-9 / (t * 1e-3) if t > 0 else None}
-                             for k, t in zip(OPS, r["abs"]["per_op"])}},
+                             for k, t in abs_ms.items()}},
+        "no_outliers": {"workload": "the same generator without the outliers (8 sinusoids + N(0,1e-3) noise) at the "
+                                    "same shape, NOA bounds as above",
+                        "value": job_gbs(n, world, r["dense"]["ms"]), "ms_per_step": r["dense"]["ms"],
+                        "bounds_verified": r["dense"]["ok"],
+                        "stream_bytes": {"stor": r["dense"]["sizes"][0], "init": r["dense"]["sizes"][1],
+                                         "resi": r["dense"]["sizes"][3]},
+                        "ops": {k: {"ms": t, "orig_GBps": n * 1e-9 / (t * 1e-3) if t > 0 else None}
+                                for k, t in dense_ms.items()}},
         "clocks": r["clocks"],
     }
     if r["tuning"] is not None:
@@ -744,25 +811,28 @@ def main():
     if r["ref_cuda"] is not None:
         rc = r["ref_cuda"]
         if "noa" in rc:  # set beside this run's own per-operation times
-            mine_abs = {k: t for k, t in zip(OPS, r["abs"]["per_op"]) if k in alg}
+            mine_abs = {k: t for k, t in abs_ms.items() if k in alg}
             rc["cortado_b200_ms"] = {"noa": {k: op_ms[k] for k in alg}, "abs": mine_abs,
                                      "noa_reference_style": {k: r["ref_style"][k] for k in alg}}
             rc["speedup_sum_of_ops"] = {"noa": rc["noa"]["sum_ms"] / sum(op_ms[k] for k in alg),
                                         "abs": rc["abs"]["sum_ms"] / sum(mine_abs.values())}
         line["ref_cuda"] = rc
-    if not args.no_extras and world == 1:
+    if extras and world == 1:
         from cortado_b200.ops import Codec
         dev = torch.device("cuda", 0)
-        c = Codec(0)
-        line["batched"] = bench_batched(c, dev)
-        c.close()
-        torch.cuda.empty_cache()
-        line["serving"] = bench_serving(dev)
-        torch.cuda.empty_cache()
-        c = Codec(0)
-        line["chain"] = bench_chain(c, dev)
-        c.close()
-        torch.cuda.empty_cache()
+        if "batched" in extras:
+            c = Codec(0)
+            line["batched"] = bench_batched(c, dev, n_fields=args.batched_fields, max_mb=args.batched_max_mb)
+            c.close()
+            torch.cuda.empty_cache()
+        if "serving" in extras:
+            line["serving"] = bench_serving(dev)
+            torch.cuda.empty_cache()
+        if "chain" in extras:
+            c = Codec(0)
+            line["chain"] = bench_chain(c, dev)
+            c.close()
+            torch.cuda.empty_cache()
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(r["x_host"])
     print(json.dumps(line))
