@@ -350,6 +350,18 @@ def _run_gpu(args, rank, world):
     torch.cuda.synchronize(dev)
     e2e_ok = bool(torch.equal(hbufs[0][2], fl.fin.cpu())) and bool(torch.equal(hbufs[1][2], hbufs[0][2]))
     e2e_ms = max_over_ranks(start.elapsed_time(end) / e_steps, world, dev)
+    # The same schedule with no device work between the copies: the time of
+    # the copies alone, the PCIe floor of the end-to-end step.
+    pipe0 = Pipeline(dev, flows, load, lambda i, f, s: None, store)
+    pipe0(2)
+    pipe0.sync()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    start.record(pipe0.s_in)
+    pipe0(e_steps)
+    end.record(pipe0.s_out)
+    torch.cuda.synchronize(dev)
+    copy_ms = max_over_ranks(start.elapsed_time(end) / e_steps, world, dev)
     codec.sync(stream)
     codec2.sync(stream2)
     codec2.close()
@@ -400,7 +412,7 @@ def _run_gpu(args, rank, world):
     if world == 1 and not args.no_ref_cuda:
         ref_cuda = reference_cuda_baseline(x_host)
     return dict(abs=abs_res, dense=dense_res, sms=torch.cuda.get_device_properties(dev).multi_processor_count,
-                ms=ms, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, ref_style=ref_style,
+                ms=ms, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, copy_ms=copy_ms, ref_style=ref_style,
                 ms_host=ms_host, per_op_host=per_op_host,
                 h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda, tuning=tuning)
 
@@ -784,7 +796,12 @@ def main():
         "value_host_scaled": {"value": job_gbs(n, world, r["ms_host"]), "ms_per_step": r["ms_host"],
                               "ops_ms": dict(zip(OPS, [float(v) for v in r["per_op_host"]]))},
         "e2e": {"value": world * n * 1e-9 / (r["e2e_ms"] * 1e-3), "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
-                "d2h_bytes_per_step": r["d2h"]},
+                "d2h_bytes_per_step": r["d2h"], "ms_per_step": r["e2e_ms"],
+                # the same copies on the same schedule without the device work
+                "copy_floor": {"ms_per_step": r["copy_ms"], "value": world * n * 1e-9 / (r["copy_ms"] * 1e-3),
+                               "h2d_GBps": r["h2d"] * 1e-9 / (r["copy_ms"] * 1e-3),
+                               "d2h_GBps": r["d2h"] * 1e-9 / (r["copy_ms"] * 1e-3)},
+                "frac_of_copy_floor": r["copy_ms"] / r["e2e_ms"]},
         # one kernel per operation, two for the NOA range (min/max, hand-over)
         "gpu_launches": args.steps * (len(OPS) + 1),
         "abs_mode": {"bounds_abs": {"store": ABS_STORE, "init": ABS_SRC, "resi": [ABS_SRC, ABS_DST]},
