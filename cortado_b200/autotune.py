@@ -89,6 +89,16 @@ def set_params(codec: Codec, params: dict) -> None:
             codec.set_resolver(op, bool(v["resolver"]))
 
 
+def choose(results: dict) -> tuple:
+    """The setting kept from a sweep {(ctas_per_sm, resolver): ms}: settings
+    within TIE of the fastest count as equal (the sweep's own noise), and
+    among them the most CTAs per SM wins, then the resolver on, since small
+    fields and batched launches gain from occupancy more than the tuning
+    field shows."""
+    fastest = min(results.values())
+    return max(k for k, v in results.items() if v <= fastest * (1 + TIE))
+
+
 def tune(codec: Codec, n_bytes: int = 128 << 20, ctas=(3, 4, 5, 6), reps: int = 5) -> dict:
     """Sweeps every operation's parameters on a seeded sinusoid + 0.1%
     outliers field of n_bytes at NOA 1e-4 (store), 1e-2 (init) and
@@ -124,12 +134,7 @@ def tune(codec: Codec, n_bytes: int = 128 << 20, ctas=(3, 4, 5, 6), reps: int = 
             for c in ctas:
                 codec.set_launch_ctas(op, c)
                 results[(c, resolver)] = _time(calls[op], reps)
-        # settings within TIE of the fastest count as equal (the sweep's own
-        # noise); among them the most CTAs per SM wins, then the resolver,
-        # since small fields and batched launches gain from occupancy more
-        # than the tuning field shows
-        fastest = min(results.values())
-        (c, resolver) = max((k for k, v in results.items() if v <= fastest * (1 + TIE)))
+        c, resolver = choose(results)
         ms = results[(c, resolver)]
         best[op] = {"ctas_per_sm": int(c), "resolver": int(resolver), "ms": ms,
                     "sweep_ms": {f"{k[0]}/{k[1]}": v for k, v in sorted(results.items())}}

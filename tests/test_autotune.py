@@ -1,4 +1,5 @@
-"""Autotuner: CPU tests of its cache, size classes and lookup order; on the
+"""Autotuner: CPU tests of its cache, size classes, lookup order and choice
+rule; on the
 GPU, a tuning run picks parameters for every operation, a cache hit applies
 them to a new context (launch shape and resolver change), and no setting
 changes an output byte."""
@@ -30,6 +31,16 @@ def test_lookup_prefers_cache_then_shipped_table(tmp_path, monkeypatch):
     assert autotune.lookup(0, 1 << 20) == (None, "defaults")
     autotune.save_cache({"Test GPU|le512MiB": {"store": {"ctas_per_sm": 3, "resolver": 0}}})
     assert autotune.lookup(0, 1 << 28) == ({"store": {"ctas_per_sm": 3, "resolver": 0}}, "cache")
+
+
+def test_choice_treats_near_ties_as_equal_and_prefers_occupancy():
+    # 5 CTAs per SM faster by 0.2%: a tie, 6 wins
+    assert autotune.choose({(5, 1): 0.3094, (6, 1): 0.3101, (6, 0): 0.3107, (3, 1): 0.39}) == (6, 1)
+    # faster by more than the tie: kept
+    assert autotune.choose({(5, 1): 0.300, (6, 1): 0.310}) == (5, 1)
+    # resolver on and off tied at the same CTAs: on
+    assert autotune.choose({(6, 0): 0.3100, (6, 1): 0.3102}) == (6, 1)
+    assert autotune.choose({(4, 1): 1.0}) == (4, 1)
 
 
 @pytest.mark.gpu
