@@ -1,8 +1,7 @@
 """Autotuner: CPU tests of its cache, size classes, lookup order and choice
-rule; on the
-GPU, a tuning run picks parameters for every operation, a cache hit applies
-them to a new context (launch shape and resolver change), and no setting
-changes an output byte."""
+rule; on the GPU, a tuning run picks parameters for every operation, a cache
+hit applies them to a new context (launch shape and resolver change), and no
+setting changes an output byte."""
 import json
 
 import pytest
