@@ -4,8 +4,9 @@ Every stream is compared byte for byte with the CPU oracle and every decoded
 float bit for bit, on the benchmark's own fields and bounds:
 
 * the headline flow on the 512^3 sinusoid + noise + 0.1% +-1e6 outliers field
-  (NOA store 1e-4, init 1e-2, residual 1e-2 -> 1e-4) and the same field's ABS
-  flow (store 1e-6, init 1e-3, residual 1e-3 -> 1e-5);
+  (NOA store 1e-4, init 1e-2, residual 1e-2 -> 1e-4), the same field's ABS
+  flow (store 1e-6, init 1e-3, residual 1e-3 -> 1e-5) and the NOA flow on
+  the generator without the outliers (bounds scaled on the device too);
 * the progressive chain on the 16384^2 GRF (k^-2.5): the four stored streams,
   the init stream and the five residual streams of the captured graph's
   replay, and every reconstruction;
@@ -90,6 +91,33 @@ def test_abs_flow_512_matches_oracle(codec, field_512):
     x, xn = field_512
     ebs = [float(storage.f32(e)) for e in (bench.ABS_STORE, bench.ABS_SRC, bench.ABS_DST)]
     _flow(codec, x, xn, *ebs)
+
+
+def test_no_outlier_noa_flow_512_matches_oracle(codec, cuda_device):
+    """The bench's no-outlier flow: the same generator without the outliers
+    at 512^3, the same NOA bounds, the bounds scaled on the device."""
+    import bench
+    x = bench.make_field(2, cuda_device, outliers=False)
+    xn = x.cpu().numpy()
+    mm = codec.INOA_find_range_device(x)
+    rng = O.noa_range(xn)
+    assert storage.value_range(*mm.cpu().tolist()) == rng
+    ebs = [float(storage.noa_scale(e, rng)) for e in (bench.EB_STORE, bench.EB_SRC, bench.EB_DST)]
+    sizes = _flow(codec, x, xn, *ebs)
+    n = x.numel() * 4
+    # the device-scaled entry points write the same streams
+    from cortado_b200.ops import max_stream_bytes
+    sz = torch.zeros(3, dtype=torch.int64, device=cuda_device)
+    stor = torch.empty(max_stream_bytes(n), dtype=torch.uint8, device=cuda_device)
+    init = torch.empty_like(stor)
+    resi = torch.empty_like(stor)
+    codec.server_encode_noa(x, n, stor, sz[0:1], mm, float(storage.f32(bench.EB_STORE)))
+    codec.s2c_encode_noa(stor, init, sz[1:2], mm, float(storage.f32(bench.EB_SRC)), n)
+    codec.residual_encode_noa(stor, resi, sz[2:3], mm, float(storage.f32(bench.EB_SRC)),
+                              float(storage.f32(bench.EB_DST)), n)
+    codec.sync()
+    assert sz.cpu().tolist() == [sizes[0], sizes[1], sizes[2]]
+    assert u8(stor[:sizes[0]]) == O.store_encode(xn, ebs[0])
 
 
 def test_chain_16384_graph_streams_match_oracle(codec, cuda_device):
