@@ -51,6 +51,8 @@ EB_STORE, EB_SRC, EB_DST = "1e-4", "1e-2", "1e-4"
 ABS_STORE, ABS_SRC, ABS_DST = "1e-6", "1e-3", "1e-5"
 OPS = ("noa_range", "store", "init_send", "init_recv", "resi_send", "resi_recv")
 FIVE = OPS[1:]  # the encode/decode operations (the reference's binaries time these)
+# the step with each send fused with the client's receive
+FUSED_OPS = ("noa_range", "store", "init_send_apply", "resi_send_apply")
 
 
 def make_field(seed: int, device, shape=SHAPE, outliers: bool = True) -> torch.Tensor:
@@ -131,10 +133,12 @@ class Flow:
     to the host, which scales the bounds, as the reference's drivers do."""
 
     def __init__(self, codec, x: torch.Tensor, stream: torch.cuda.Stream, abs_mode: bool = False,
-                 device_noa: bool = True):
+                 device_noa: bool = True, fused: bool = False):
         from cortado_b200 import ops
         self.c, self.x, self.s, self.abs_mode = codec, x, stream, abs_mode
         self.device_noa = device_noa
+        self.fused = fused  # NOA, device bounds: sends fused with the receives (the client's floats in fin)
+        self.ops = FUSED_OPS if fused else OPS
         self.mm = torch.empty(2, dtype=torch.float32, device=x.device)
         self.stream = stream  # the compute stream, as cortado_b200.pipeline expects
         dev = x.device
@@ -146,7 +150,7 @@ class Flow:
         self.cl = torch.empty_like(x)
         self.fin = torch.empty_like(x)
         self.sizes = torch.zeros(8, dtype=torch.int64, device=dev)
-        self.ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(OPS) + 1)]
+        self.ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(self.ops) + 1)]
 
     def bounds(self):
         from cortado_b200 import storage
@@ -190,6 +194,15 @@ class Flow:
         rec(0)
         c.INOA_find_range_device(self.x, mm, stream=s)  # computed in both modes, as the reference's store does
         rec(1)
+        if self.fused:
+            a, b, d = (float(storage.f32(e)) for e in (EB_STORE, EB_SRC, EB_DST))
+            c.server_encode_noa(self.x, self.n, self.stor, sz[0:1], mm, a, stream=s)
+            rec(2)
+            c.s2c_encode_apply_noa(self.stor, self.init, sz[1:2], mm, b, self.n, self.fin, stream=s)
+            rec(3)
+            c.residual_encode_apply_noa(self.stor, self.resi, sz[3:4], mm, b, d, self.n, self.fin, stream=s)
+            rec(4)
+            return
         if self.abs_mode:
             a, b, d = (float(storage.f32(e)) for e in (ABS_STORE, ABS_SRC, ABS_DST))
             c.server_encode(self.x, self.n, self.stor, sz[0:1], a, stream=s)
@@ -213,7 +226,7 @@ class Flow:
         rec(6)
 
     def op_ms(self):
-        return [self.ev[i].elapsed_time(self.ev[i + 1]) for i in range(len(OPS))]
+        return [self.ev[i].elapsed_time(self.ev[i + 1]) for i in range(len(self.ops))]
 
 
 def run_gpu(args, rank, world):
@@ -256,7 +269,7 @@ def _run_gpu(args, rank, world):
         """k steps enqueued back to back (the device-NOA flow waits for nothing
         on the host), each with its own events; returns (ms per step, mean ms
         per operation)."""
-        sets = [[torch.cuda.Event(enable_timing=True) for _ in range(len(OPS) + 1)] for _ in range(k)]
+        sets = [[torch.cuda.Event(enable_timing=True) for _ in range(len(flow.ops) + 1)] for _ in range(k)]
         st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(flow.s):
             st.record(flow.s)
@@ -265,7 +278,7 @@ def _run_gpu(args, rank, world):
                 flow.step(timed=True)
             en.record(flow.s)
             torch.cuda.synchronize(dev)
-        ops = np.mean([[e[i].elapsed_time(e[i + 1]) for i in range(len(OPS))] for e in sets], axis=0)
+        ops = np.mean([[e[i].elapsed_time(e[i + 1]) for i in range(len(flow.ops))] for e in sets], axis=0)
         return st.elapsed_time(en) / k, ops
 
     ms, per_op = timed_steps(fl, args.steps)
@@ -282,6 +295,21 @@ def _run_gpu(args, rank, world):
     codec.sync(stream)
     ms_host = max_over_ranks(ms_host, world, dev)
     del fh
+    # the same step with each send fused with the client's receive (a server
+    # that keeps the client's reconstruction on this GPU): four launches, the
+    # same streams and the same final reconstruction
+    ff = Flow(codec, x, stream, fused=True)
+    with torch.cuda.stream(stream):
+        ff.step()
+        codec.sync(stream)
+    s_i, s_r = int(fl.sizes[1]), int(fl.sizes[3])
+    fused_ok = (int(ff.sizes[1]) == s_i and int(ff.sizes[3]) == s_r and torch.equal(ff.init[:s_i], fl.init[:s_i])
+                and torch.equal(ff.resi[:s_r], fl.resi[:s_r])
+                and torch.equal(ff.fin.view(torch.int32), fl.fin.view(torch.int32)))
+    ms_fused, per_op_fused = timed_steps(ff, args.steps)
+    codec.sync(stream)
+    ms_fused = max_over_ranks(ms_fused, world, dev)
+    del ff
 
     # Reference-style timing of each operation: the host clock around one call
     # and a stream synchronize, median of 10 after a warm-up, as the
@@ -414,7 +442,8 @@ def _run_gpu(args, rank, world):
         ref_cuda = reference_cuda_baseline(x_host)
     return dict(abs=abs_res, dense=dense_res, sms=torch.cuda.get_device_properties(dev).multi_processor_count,
                 ms=ms, per_op=per_op, n=n, sizes=sizes, ok=ok, e2e_ms=e2e_ms, copy_ms=copy_ms, ref_style=ref_style,
-                ms_host=ms_host, per_op_host=per_op_host,
+                ms_host=ms_host, per_op_host=per_op_host, ms_fused=ms_fused, per_op_fused=per_op_fused,
+                fused_ok=fused_ok,
                 h2d=n, d2h=s_init + s_resi + n, x_host=x_host, ref_cuda=ref_cuda, tuning=tuning)
 
 
@@ -793,6 +822,12 @@ def main():
                      "per_kernel_frac_no_outliers": dense_fracs,
                      # the re-encoders' own bound: the fraction of the SMs' issue rate
                      "issue_frac": issue_fracs(n, op_ms, r["sms"], r["clocks"].get("sm_mhz"))},
+        "fused_flow": {"what": "the same step with init_send and resi_send each fused with the client's receive "
+                               "(the client's reconstruction kept on this GPU): range, store, init_send_apply, "
+                               "resi_send_apply",
+                       "value": job_gbs(n, world, r["ms_fused"]), "ms_per_step": r["ms_fused"],
+                       "ops_ms": dict(zip(FUSED_OPS, [float(v) for v in r["per_op_fused"]])),
+                       "matches_plain": r["fused_ok"]},
         # the same flow with the range handed to the host for the bounds' scaling
         "value_host_scaled": {"value": job_gbs(n, world, r["ms_host"]), "ms_per_step": r["ms_host"],
                               "ops_ms": dict(zip(OPS, [float(v) for v in r["per_op_host"]]))},

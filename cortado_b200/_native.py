@@ -47,6 +47,8 @@ SIGNATURES = {
     "cortado_init_send_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _vp, _i64, _vp, _vp]),
     "cortado_resi_send_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _f32, _vp, _i64, _vp, _vp]),
     "cortado_resi_send_apply": (_int, [_vp, _vp, _i64, _i64, _f32, _f32, _vp, _i64, _vp, _vp, _vp]),
+    "cortado_init_send_apply_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _vp, _i64, _vp, _vp, _vp]),
+    "cortado_resi_send_apply_noa": (_int, [_vp, _vp, _i64, _i64, _vp, _f32, _f32, _vp, _i64, _vp, _vp, _vp]),
 }
 
 OPS = {"store": 0, "init_send": 1, "resi_send": 2, "store_decode": 3, "init_recv": 4, "resi_recv": 5,

@@ -519,32 +519,86 @@ __device__ __forceinline__ void store_loop(Ctl& sm, const Src& src, const Sync& 
 //         (client_raw_bins), as init_recv copies raw chunks out as stored;
 //   resi: iCQ(CQ(client, dst) + residual, dst) (d_RESI_4.h:79-94); the
 //         residual ints are the same whether the chunk compresses or not.
-// Thread g handles its group's 32 words, 16 bytes at a time (the client's
-// words are read and written in place); forms as in the decoders, chosen per
-// word.
+// A full chunk goes through the stage buffer X, whose rows 32w .. 32w+31
+// only warp w touches at this point of the loop (row tid is each thread's
+// own): the warp moves its 4 KiB of the client's floats between global and
+// those rows 512 contiguous bytes at a time, and each thread works on its own
+// row.  The float forms apply when the whole warp allows them (no lossless
+// client word, no lossless bin), else the per-word forms, as in the decoders.
+// A partial chunk works word by word on the client's floats directly.
 template <int OP>
-__device__ __forceinline__ void client_apply(const OpArgs& A, long long c, int nw, const uint32_t (&v)[32], Quant q) {
-  const int tid = threadIdx.x;
+__device__ __forceinline__ void client_apply(const OpArgs& A, long long c, int nw, const uint32_t (&v)[32], Quant q,
+                                             uint32_t* X) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const FastQ fq = make_fastq(q.eb_e);
-  uint32_t* row = reinterpret_cast<uint32_t*>(A.client) + c * (long long)CW + 32 * tid;
   if (nw == CW) {
-    uint4* r4 = reinterpret_cast<uint4*>(row);
+    uint4* g4 = reinterpret_cast<uint4*>(A.client) + c * (long long)(CW / 4) + 256 * warp;
+    uint4* X4 = reinterpret_cast<uint4*>(X);
+    uint4* own = X4 + 8 * tid;
+    // lane l's part of the warp's i-th 512 bytes: linear 16-byte unit
+    // 256*warp + 32*i + l, i.e. row 32*warp + 4*i + l/8, unit l%8 of that row
+    auto unit = [&](int i) -> uint4* {
+      const int r = 32 * warp + 4 * i + (lane >> 3);
+      return X4 + 8 * r + ((lane & 7) ^ (r & 7));
+    };
+    __syncwarp();  // the rows' earlier uses by this warp's threads are done
+    uint32_t bmax = 0;
+    if (OP == OP_S2C) {
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        const uint32_t neg = (uint32_t)((int32_t)v[k] >> 31);
+        bmax = max(bmax, (v[k] ^ neg) - neg);
+      }
+    } else {
+#pragma unroll 2  // (fully unrolled, eight 16-byte loads in flight beside v spill)
+      for (int i = 0; i < 8; i++) *unit(i) = g4[32 * i + lane];
+      __syncwarp();
+      uint32_t amax = 0;
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint4 w = own[u ^ (tid & 7)];
+        amax = max(amax, max(max(w.x & 0x7fffffffu, w.y & 0x7fffffffu), max(w.z & 0x7fffffffu, w.w & 0x7fffffffu)));
+      }
+      // destination bins of the client's floats plus the residuals, into the row
+      const bool fast_c = !__any_sync(0xffffffffu, amax >= fq.thr_bits);
+      __syncwarp();  // the row is read again below, not held in registers beside v
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint4 w = own[u ^ (tid & 7)];
+        uint4 b;
+        if (fast_c) {
+          b = make_uint4(cq_fast(w.x, fq) + v[4 * u], cq_fast(w.y, fq) + v[4 * u + 1], cq_fast(w.z, fq) + v[4 * u + 2],
+                         cq_fast(w.w, fq) + v[4 * u + 3]);
+        } else {
+          b = make_uint4(cq_mixed(w.x, fq, q) + v[4 * u], cq_mixed(w.y, fq, q) + v[4 * u + 1],
+                         cq_mixed(w.z, fq, q) + v[4 * u + 2], cq_mixed(w.w, fq, q) + v[4 * u + 3]);
+        }
+        own[u ^ (tid & 7)] = b;
+        const uint32_t b4[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const uint32_t neg = (uint32_t)((int32_t)b4[j] >> 31);
+          bmax = max(bmax, (b4[j] ^ neg) - neg);
+        }
+      }
+    }
+    // dequantized bins into the row
+    const bool fast_i = __all_sync(0xffffffffu, bmax < 0x800000u);
+    __syncwarp();  // as above: the bins are read back from the row
 #pragma unroll
     for (int u = 0; u < 8; u++) {
-      uint4 o;
-      if (OP == OP_S2C) {
-        o = make_uint4(iq_mixed(v[4 * u], fq, q), iq_mixed(v[4 * u + 1], fq, q), iq_mixed(v[4 * u + 2], fq, q),
-                       iq_mixed(v[4 * u + 3], fq, q));
-      } else {
-        const uint4 w = r4[u];
-        o = make_uint4(iq_mixed(cq_mixed(w.x, fq, q) + v[4 * u], fq, q),
-                       iq_mixed(cq_mixed(w.y, fq, q) + v[4 * u + 1], fq, q),
-                       iq_mixed(cq_mixed(w.z, fq, q) + v[4 * u + 2], fq, q),
-                       iq_mixed(cq_mixed(w.w, fq, q) + v[4 * u + 3], fq, q));
-      }
-      r4[u] = o;
+      const uint4 b = (OP == OP_S2C) ? make_uint4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3])
+                                     : own[u ^ (tid & 7)];
+      own[u ^ (tid & 7)] = fast_i ? make_uint4(iq_fast(b.x, fq), iq_fast(b.y, fq), iq_fast(b.z, fq), iq_fast(b.w, fq))
+                                  : make_uint4(iq_mixed(b.x, fq, q), iq_mixed(b.y, fq, q), iq_mixed(b.z, fq, q),
+                                               iq_mixed(b.w, fq, q));
     }
+    __syncwarp();
+#pragma unroll 2
+    for (int i = 0; i < 8; i++) g4[32 * i + lane] = *unit(i);
+    __syncwarp();  // the rows are read before the encoder reuses the buffer
   } else {
+    uint32_t* row = reinterpret_cast<uint32_t*>(A.client) + c * (long long)CW + 32 * tid;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
       if (32 * tid + k < nw) {
@@ -582,7 +636,9 @@ __device__ __noinline__ void raw_rebuild(Ctl& sm, const uint32_t* X, int nw, uin
 // (as in store_loop).  A chunk that does not compress stores its requantized
 // words, which are rebuilt from the plane buffer (planes_to_words) into
 // buffer 1 -- rare enough not to keep a third buffer for them.
-template <int OP, class Src>
+// APPLY: the fused send-and-apply forms (items with a client's floats); the
+// plain forms are compiled without that code.
+template <int OP, bool APPLY, class Src>
 __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Sync& sy) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   begin_launch(sm, sy);
@@ -604,7 +660,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       long long g = 0;
       if (lane == 0) g = atomicAdd(&sy.counter[0], 1u);
       prefetch_stream(sm, 0, __shfl_sync(0xffffffffu, g, 0), src, ws);
-      if (OP == OP_RESI && lane == 0) {
+      if (OP == OP_RESI && APPLY && lane == 0) {
         // resi_send with apply reads the client's chunk: bring it into L2 now
         const StageMeta& mn = sm.st[0];
         if (mn.g < src.total && mn.bad == 0) {
@@ -683,7 +739,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
         row_load(X, tid, v);
       }
       if (Src::batched && c == 0 && tid == 0) write_header(A.out, m.n, (OP == OP_S2C) ? q1.eb_e : q2.eb_e);
-      if (A.client) client_apply<OP>(A, c, nw, v, OP == OP_S2C ? q1 : q2);
+      if (APPLY && A.client) client_apply<OP>(A, c, nw, v, OP == OP_S2C ? q1 : q2, X);
       if (nw == CW) {
         encode_stage<true>(sm, A.sy, v, X, Y, c, nw, item, sm.pend[s], flush_prev);
       } else {
@@ -695,7 +751,7 @@ __device__ __forceinline__ void reencode_loop(Ctl& sm, const Src& src, const Syn
       if (sm.pend[s].raw) {
         // the requantized words, rebuilt from the plane buffer, are the payload
         raw_rebuild(sm, X, nw, Yw);
-        if (OP == OP_S2C && A.client) client_raw_bins(A, c, nw, Yw);
+        if (OP == OP_S2C && APPLY && A.client) client_raw_bins(A, c, nw, Yw);
       }
     }
     if (tid == 0) sm.pend[s ^ 1].valid = 0;
@@ -927,7 +983,7 @@ __global__ void __launch_bounds__(NT, MINB_STORE) k_store(const __grid_constant_
   finish_launch(sm, a.sy);
 }
 
-template <int OP>
+template <int OP, bool APPLY>
 __global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_constant__ OpArgs a) {
   Ctl& sm = ctl_block();
   StreamHdr h = read_header(a.in, a.in_bytes);
@@ -947,7 +1003,7 @@ __global__ void __launch_bounds__(NT, MINB_REENC) k_reencode(const __grid_consta
   }
   const SingleSrc src{&a, nullptr, nullptr, h.chunks, h, q1, q2};
   if (helper_cta(sm, a.sy)) run_helper<true, true>(sm, src, a.sy);
-  else reencode_loop<OP>(sm, src, a.sy);
+  else reencode_loop<OP, APPLY>(sm, src, a.sy);
   finish_launch(sm, a.sy);
 }
 
@@ -970,7 +1026,7 @@ __global__ void __launch_bounds__(NT, OP == OP_RAPPLY ? MINB_RAPPLY : MINB_DEC) 
 }
 
 // ---- batched kernels: one persistent launch over many streams.
-template <int OP>
+template <int OP, bool APPLY = false>
 __global__ void __launch_bounds__(NT, OP == OP_STORE ? MINB_STORE : (OP == OP_RAPPLY ? MINB_RAPPLY : (OP == OP_S2C || OP == OP_RESI) ? MINB_REENC : MINB_DEC))
 k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks, const __grid_constant__ Sync sy) {
   Ctl& sm = ctl_block();
@@ -978,7 +1034,7 @@ k_batch(const BatchItem* __restrict__ items, int n_items, long long total_chunks
   constexpr bool encoder = OP == OP_STORE || OP == OP_S2C || OP == OP_RESI;
   if (helper_cta(sm, sy)) run_helper<encoder, OP != OP_STORE>(sm, src, sy);
   else if (OP == OP_STORE) store_loop(sm, src, sy);
-  else if (encoder) reencode_loop<OP>(sm, src, sy);
+  else if (encoder) reencode_loop<OP, APPLY>(sm, src, sy);
   else decode_loop<OP>(sm, src, sy);
   finish_launch(sm, sy);
 }
@@ -1309,14 +1365,18 @@ cortado_status cortado_create(cortado_ctx** out, int device) {
   e = cudaHostAlloc((void**)&ctx->h_range, 8, cudaHostAllocMapped);
   if (e != cudaSuccess) { cudaFree(ctx->words); delete ctx; return from_cuda(e); }
   ctx->grid_store = occupancy_grid(k_store, SMEM_STD, ctx->sms);
-  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C>, SMEM_STD, ctx->sms);
-  occupancy_grid(k_reencode<OP_RESI>, SMEM_STD, ctx->sms);
+  ctx->grid_reenc = occupancy_grid(k_reencode<OP_S2C, false>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_reencode<OP_RESI, false>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_reencode<OP_S2C, true>, SMEM_STD, ctx->sms);  // the fused forms
+  occupancy_grid(k_reencode<OP_RESI, true>, SMEM_STD, ctx->sms);
   ctx->grid_dec = occupancy_grid(k_decode<OP_SDEC>, SMEM_STD, ctx->sms);
   occupancy_grid(k_decode<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_rapply = occupancy_grid(k_decode<OP_RAPPLY>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_STORE] = occupancy_grid(k_batch<OP_STORE>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_S2C] = occupancy_grid(k_batch<OP_S2C>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RESI] = occupancy_grid(k_batch<OP_RESI>, SMEM_STD, ctx->sms);
+  occupancy_grid(k_batch<OP_S2C, true>, SMEM_STD, ctx->sms);  // the fused forms: same shape, attributes set
+  occupancy_grid(k_batch<OP_RESI, true>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_SDEC] = occupancy_grid(k_batch<OP_SDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_CDEC] = occupancy_grid(k_batch<OP_CDEC>, SMEM_STD, ctx->sms);
   ctx->grid_batch[OP_RAPPLY] = occupancy_grid(k_batch<OP_RAPPLY>, SMEM_STD, ctx->sms);
@@ -1448,8 +1508,10 @@ static cortado_status reencode(cortado_ctx* ctx, int op, const void* d_stored, i
   a.client = (uint8_t*)d_client;
   a.sy = next_sync(ctx, st, op);
   const int grid = grid_for(tuned_grid(ctx, op, ctx->grid_reenc), chunks);
-  if (op == OP_S2C) k_reencode<OP_S2C><<<grid, NT, SMEM_STD, st>>>(a);
-  else k_reencode<OP_RESI><<<grid, NT, SMEM_STD, st>>>(a);
+  if (op == OP_S2C && d_client) k_reencode<OP_S2C, true><<<grid, NT, SMEM_STD, st>>>(a);
+  else if (op == OP_S2C) k_reencode<OP_S2C, false><<<grid, NT, SMEM_STD, st>>>(a);
+  else if (d_client) k_reencode<OP_RESI, true><<<grid, NT, SMEM_STD, st>>>(a);
+  else k_reencode<OP_RESI, false><<<grid, NT, SMEM_STD, st>>>(a);
   return launch_status(cudaSuccess);
 }
 
@@ -1538,6 +1600,24 @@ cortado_status cortado_resi_send_noa(cortado_ctx* ctx, const void* d_stored, int
   if (!d_minmax) return CORTADO_ERR_INVALID_ARG;
   return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_noa, dst_eb_noa, d_out, out_capacity,
                   d_outsize, stream, nullptr, d_minmax);
+}
+
+cortado_status cortado_init_send_apply_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                           const float* d_minmax, float request_eb_noa, void* d_out,
+                                           int64_t out_capacity, int64_t* d_outsize, void* d_client,
+                                           cortado_stream_t stream) {
+  if (!d_minmax || (!d_client && n_bytes)) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_S2C, d_stored, stored_bytes, n_bytes, request_eb_noa, 0.0f, d_out, out_capacity, d_outsize,
+                  stream, d_client, d_minmax);
+}
+
+cortado_status cortado_resi_send_apply_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                           const float* d_minmax, float src_eb_noa, float dst_eb_noa, void* d_out,
+                                           int64_t out_capacity, int64_t* d_outsize, void* d_client,
+                                           cortado_stream_t stream) {
+  if (!d_minmax || (!d_client && n_bytes)) return CORTADO_ERR_INVALID_ARG;
+  return reencode(ctx, OP_RESI, d_stored, stored_bytes, n_bytes, src_eb_noa, dst_eb_noa, d_out, out_capacity,
+                  d_outsize, stream, d_client, d_minmax);
 }
 
 static cortado_status decode(cortado_ctx* ctx, int op, const void* d_stream, int64_t stream_bytes, const void* d_src,
@@ -1717,8 +1797,14 @@ cortado_status cortado_batch(cortado_ctx* ctx, cortado_op op, const cortado_item
   const size_t smem = (op == CORTADO_OP_RESI_RECV) ? SMEM_STD : SMEM_STD;
   switch (op) {
     case CORTADO_OP_STORE: k_batch<OP_STORE><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
-    case CORTADO_OP_INIT_SEND: k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
-    case CORTADO_OP_RESI_SEND: k_batch<OP_RESI><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
+    case CORTADO_OP_INIT_SEND:
+      if (apply) k_batch<OP_S2C, true><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy);
+      else k_batch<OP_S2C><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy);
+      break;
+    case CORTADO_OP_RESI_SEND:
+      if (apply) k_batch<OP_RESI, true><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy);
+      else k_batch<OP_RESI><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy);
+      break;
     case CORTADO_OP_STORE_DECODE: k_batch<OP_SDEC><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
     case CORTADO_OP_INIT_RECV: k_batch<OP_CDEC><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;
     case CORTADO_OP_RESI_RECV: k_batch<OP_RAPPLY><<<grid, NT, smem, st>>>(d_tab, n_items, total, sy); break;

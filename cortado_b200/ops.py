@@ -204,6 +204,25 @@ class Codec:
                                             _nbytes(d_output), _ptr(d_outsize), _stream(stream)),
               "residual_encode_noa")
 
+    def s2c_encode_apply_noa(self, d_input, d_output, d_outsize, d_minmax, request_eb_noa, n_bytes, d_client,
+                             in_bytes=None, stream=None):
+        """s2c_encode_apply at a NOA request bound of the device range."""
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_init_send_apply_noa(self._h, _ptr(d_input), n, int(n_bytes), _ptr(d_minmax),
+                                                  float(request_eb_noa), _ptr(d_output), _nbytes(d_output),
+                                                  _ptr(d_outsize), _ptr(d_client), _stream(stream)),
+              "s2c_encode_apply_noa")
+
+    def residual_encode_apply_noa(self, d_input, d_output, d_outsize, d_minmax, src_eb_noa, dest_eb_noa, n_bytes,
+                                  d_client, in_bytes=None, stream=None):
+        """residual_encode_apply between NOA bounds of the device range."""
+        n = _nbytes(d_input) if in_bytes is None else int(in_bytes)
+        check(self._L.cortado_resi_send_apply_noa(self._h, _ptr(d_input), n, int(n_bytes), _ptr(d_minmax),
+                                                  float(src_eb_noa), float(dest_eb_noa), _ptr(d_output),
+                                                  _nbytes(d_output), _ptr(d_outsize), _ptr(d_client),
+                                                  _stream(stream)),
+              "residual_encode_apply_noa")
+
     def verify_bound(self, orig, recon, eb_abs, first_bad=None, stream=None):
         """MAXABS_f32 on the device: returns the int64 tensor holding the first
         violating index (or -1 when every value is within eb_abs)."""

@@ -167,6 +167,20 @@ cortado_status cortado_resi_send_noa(cortado_ctx* ctx, const void* d_stored, int
                                      const float* d_minmax, float src_eb_noa, float dst_eb_noa, void* d_out,
                                      int64_t out_capacity, int64_t* d_outsize, cortado_stream_t stream);
 
+/* init_send / resi_send fused with the client's receive (as
+ * cortado_init_send_apply / cortado_resi_send_apply) at NOA bounds of the
+ * range in d_minmax: the stream and the client's reconstruction are
+ * byte-identical to the host-scaled fused calls; on a latched bound error
+ * neither is written. */
+cortado_status cortado_init_send_apply_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                           const float* d_minmax, float request_eb_noa, void* d_out,
+                                           int64_t out_capacity, int64_t* d_outsize, void* d_client,
+                                           cortado_stream_t stream);
+cortado_status cortado_resi_send_apply_noa(cortado_ctx* ctx, const void* d_stored, int64_t stored_bytes, int64_t n_bytes,
+                                           const float* d_minmax, float src_eb_noa, float dst_eb_noa, void* d_out,
+                                           int64_t out_capacity, int64_t* d_outsize, void* d_client,
+                                           cortado_stream_t stream);
+
 /* Bound verifier: writes to *d_first_bad (device) the first index i at which
  * recon[i] violates |orig[i] - recon[i]| <= eb_abs under the reference's
  * MAXABS_f32 rules (include/verifiers/MAXABS_f32.h:40-72; NaN and Inf must

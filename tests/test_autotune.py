@@ -35,8 +35,9 @@ def test_lookup_prefers_cache_then_shipped_table(tmp_path, monkeypatch):
 def test_choice_treats_near_ties_as_equal_and_prefers_occupancy():
     # 5 CTAs per SM faster by 0.2%: a tie, 6 wins
     assert autotune.choose({(5, 1): 0.3094, (6, 1): 0.3101, (6, 0): 0.3107, (3, 1): 0.39}) == (6, 1)
+    assert autotune.choose({(5, 1): 0.3046, (6, 1): 0.3078, (6, 0): 0.3108}) == (6, 1)
     # faster by more than the tie: kept
-    assert autotune.choose({(5, 1): 0.300, (6, 1): 0.310}) == (5, 1)
+    assert autotune.choose({(5, 1): 0.300, (6, 1): 0.320}) == (5, 1)
     # resolver on and off tied at the same CTAs: on
     assert autotune.choose({(6, 0): 0.3100, (6, 1): 0.3102}) == (6, 1)
     assert autotune.choose({(4, 1): 1.0}) == (4, 1)

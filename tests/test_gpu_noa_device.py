@@ -1,5 +1,6 @@
 """NOA bounds scaled on the device (cortado_noa_range_device and the
-cortado_*_noa entry points): the streams are byte-identical to the
+cortado_*_noa entry points, the fused send-and-apply forms included): the
+streams and client reconstructions are byte-identical to the
 host-scaled calls with the drivers' float arithmetic (storage.noa_scale of
 the device range), bound errors are latched and written nowhere, and a whole
 NOA flow is captured in a CUDA graph and replayed with identical results
@@ -62,6 +63,39 @@ def test_device_noa_equals_host_scaled(codec, name, x):
         assert u8(resi[: int(sz[2].item())]) == u8(codec.resi_send(ref, ea, eb)) == O.resi_send(u8(ref), ea, eb)
 
 
+@pytest.mark.parametrize("name,x", _fields(), ids=[n for n, _ in _fields()])
+def test_fused_device_noa_equals_host_scaled(codec, name, x):
+    """cortado_*_send_apply_noa: stream and client reconstruction equal the
+    host-scaled fused calls' and the separate receive's."""
+    from cortado_b200.ops import max_stream_bytes
+    xg = torch.from_numpy(x).cuda()
+    n = x.size * 4
+    mm = codec.INOA_find_range_device(xg)
+    rng = storage.value_range(*mm.cpu().tolist())
+    cap = max_stream_bytes(n)
+    sz = torch.zeros(4, dtype=torch.int64, device="cuda")
+    stor = codec.store(xg, float(storage.noa_scale(1e-5, rng)))
+    req, dst = 1e-2, 1e-4
+    ea, eb = float(storage.noa_scale(req, rng)), float(storage.noa_scale(dst, rng))
+    init, init_h = (torch.empty(cap, dtype=torch.uint8, device="cuda") for _ in range(2))
+    cl, cl_h = torch.full_like(xg, 7.0), torch.full_like(xg, -7.0)
+    codec.s2c_encode_apply_noa(stor, init, sz[0:1], mm, req, n, cl)
+    codec.s2c_encode_apply(stor, init_h, sz[1:2], ea, n, cl_h)
+    codec.sync()
+    assert int(sz[0]) == int(sz[1]) and u8(init[: int(sz[0])]) == u8(init_h[: int(sz[1])])
+    assert torch.equal(cl.view(torch.int32), cl_h.view(torch.int32))
+    assert torch.equal(cl.view(torch.int32), codec.init_recv(init[: int(sz[0])]).view(torch.int32))
+    before = cl.clone()
+    resi, resi_h = (torch.empty(cap, dtype=torch.uint8, device="cuda") for _ in range(2))
+    codec.residual_encode_apply_noa(stor, resi, sz[2:3], mm, req, dst, n, cl)
+    codec.residual_encode_apply(stor, resi_h, sz[3:4], ea, eb, n, cl_h)
+    codec.sync()
+    assert int(sz[2]) == int(sz[3]) and u8(resi[: int(sz[2])]) == u8(resi_h[: int(sz[3])])
+    assert u8(resi[: int(sz[2])]) == O.resi_send(u8(stor), ea, eb)
+    assert torch.equal(cl.view(torch.int32), cl_h.view(torch.int32))
+    assert torch.equal(cl.view(torch.int32), codec.resi_recv(before, resi[: int(sz[2])]).view(torch.int32))
+
+
 def test_device_noa_bound_errors_are_latched(codec):
     from cortado_b200._native import CortadoError
     from cortado_b200.ops import max_stream_bytes
@@ -81,6 +115,14 @@ def test_device_noa_bound_errors_are_latched(codec):
     with pytest.raises(CortadoError) as e:
         codec.sync()
     assert e.value.name == "EB_TOO_LARGE"
+    # the fused forms latch the same error and write neither the stream nor the client
+    cl = torch.full_like(y, 5.0)
+    stor = codec.store(y, 1e-3)
+    codec.s2c_encode_apply_noa(stor, out, sz, mm, 3e38, y.numel() * 4, cl)
+    with pytest.raises(CortadoError) as e:
+        codec.sync()
+    assert e.value.name == "EB_TOO_LARGE"
+    assert int(sz.item()) == -7 and bool((out == 0x5A).all()) and bool((cl == 5.0).all())
     codec.server_encode_noa(y, y.numel() * 4, out, sz, mm, 1e-3)  # the context stays usable
     codec.sync()
     assert int(sz.item()) > 0
