@@ -550,8 +550,9 @@ __device__ __forceinline__ void client_apply(const OpArgs& A, long long c, int n
         bmax = max(bmax, (v[k] ^ neg) - neg);
       }
     } else {
-#pragma unroll 2  // (fully unrolled, eight 16-byte loads in flight beside v spill)
-      for (int i = 0; i < 8; i++) *unit(i) = g4[32 * i + lane];
+#pragma unroll
+      for (int i = 0; i < 8; i++) async_copy16(unit(i), g4 + 32 * i + lane);  // all eight in flight, no registers
+      async_wait_all();
       __syncwarp();
       uint32_t amax = 0;
 #pragma unroll

@@ -155,6 +155,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// 16 bytes from global to shared memory without a register round trip
+// (the thread's own copies complete at async_wait_all); both addresses
+// 16-byte aligned.
+__device__ __forceinline__ void async_copy16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---------------------------------------------------------------- status
 __device__ __forceinline__ void latch(unsigned int* status, unsigned int code) {
   atomicCAS(status, 0u, code);

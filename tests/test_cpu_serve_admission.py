@@ -2,7 +2,8 @@
 the GPU launches are replaced by fakes whose completion events report done
 after a few polls.  Checked: a client's steps on a field start only after its
 previous step finished and in arrival order; batches hold at most max_batch
-requests; at most max_inflight requests are in flight; the memory cap holds,
+requests; at most max_inflight requests (and, when set, max_batches batches)
+are in flight; the memory cap holds,
 counting reconstructions and pooled output buffers; a client held back by its
 own running step does not hold back other clients; idle state is spilled to
 host files and read back unchanged; a request larger than the memory cap is
@@ -29,7 +30,7 @@ class _Codec:
         pass
 
 
-def _server(sizes, max_inflight, max_batch, mem_cap, polls=3, stored_bytes=0, spill_dir=None):
+def _server(sizes, max_inflight, max_batch, mem_cap, polls=3, stored_bytes=0, spill_dir=None, max_batches=None):
     srv = serve.Server.__new__(serve.Server)
     srv.dev = torch.device("cpu")
     srv.codecs = [_Codec() for _ in range(3)]
@@ -37,6 +38,7 @@ def _server(sizes, max_inflight, max_batch, mem_cap, polls=3, stored_bytes=0, sp
     srv.mem_cap = mem_cap
     srv.max_inflight = max_inflight
     srv.max_batch = max_batch
+    srv.max_batches = max_batches
     srv.fields = {name: serve.Field(name, torch.zeros(n // 4), [1.0]) for name, n in sizes.items()}
     srv.clients = {}
     srv.mem_used = 0
@@ -47,7 +49,7 @@ def _server(sizes, max_inflight, max_batch, mem_cap, polls=3, stored_bytes=0, sp
         f.stored = [torch.arange(stored_bytes, dtype=torch.int64).to(torch.uint8)] if stored_bytes else []
         f.stored_bytes = [stored_bytes] if stored_bytes else []
         srv.mem_used += stored_bytes
-    launches, launched = [], []
+    launches, launched, batches = [], [], []
     recon_of = {}
 
     def fake_launch(k, reqs):
@@ -63,9 +65,11 @@ def _server(sizes, max_inflight, max_batch, mem_cap, polls=3, stored_bytes=0, sp
             st["bound"] = r.bound
         launches.append({"stream": k, "rids": [r.rid for r in reqs],
                          "inflight": sum(1 for r in launched if r.done < 0),
+                         "batches_inflight": sum(1 for b in batches if any(r.done < 0 for r in b)),
                          "mem_used": srv.mem_used,
                          "prev_done": [all(p.done >= 0 for p in launched[:-len(reqs)]
                                            if (p.client, p.field) == (r.client, r.field)) for r in reqs]})
+        batches.append(list(reqs))
         return _Event(polls), outs, None
 
     srv._launch = fake_launch
@@ -107,6 +111,23 @@ def test_admission_invariants(rate_hz, max_batch, max_inflight):
     for rids in by_key.values():
         assert [pos[x] for x in rids] == sorted(pos[x] for x in rids)
     assert srv.mem_used == _accounted(srv)
+
+
+@pytest.mark.parametrize("max_batches", [1, 2])
+@pytest.mark.parametrize("rate_hz", [None, 5e4])
+def test_batches_in_flight_limit(rate_hz, max_batches):
+    """With max_batches set, a batch is launched only while fewer batches are
+    in flight, so the requests that arrive meanwhile gather into the next one."""
+    rng = np.random.Generator(np.random.PCG64(4))
+    sizes = {f"f{i}": int(rng.integers(1, 64)) << 16 for i in range(6)}
+    srv, launches = _server(sizes, 64, 16, 10**12, max_batches=max_batches)
+    trace = _trace(rng, sorted(sizes), 120, 8, rate_hz)
+    stats, _ = srv.run(trace)
+    assert stats["requests"] == len(trace)
+    assert all(b["batches_inflight"] < max_batches for b in launches)
+    assert sorted(rid for b in launches for rid in b["rids"]) == list(range(len(trace)))
+    if rate_hz is None:  # everything queued: full batches but for the clients' own order
+        assert max(len(b["rids"]) for b in launches) > 1
 
 
 def _accounted(srv):
