@@ -827,6 +827,11 @@ def main():
                                "resi_send_apply",
                        "value": job_gbs(n, world, r["ms_fused"]), "ms_per_step": r["ms_fused"],
                        "ops_ms": dict(zip(FUSED_OPS, [float(v) for v in r["per_op_fused"]])),
+                       # algorithmic bytes: the stored stream in, the stream out, the
+                       # client's floats written (init) or read and written (resi)
+                       "per_kernel_frac": {
+                           "init_send_apply": (s_stor + s_init + n) / (r["per_op_fused"][2] * 1e-3) * 1e-9 / peak,
+                           "resi_send_apply": (s_stor + s_resi + 2 * n) / (r["per_op_fused"][3] * 1e-3) * 1e-9 / peak},
                        "matches_plain": r["fused_ok"]},
         # the same flow with the range handed to the host for the bounds' scaling
         "value_host_scaled": {"value": job_gbs(n, world, r["ms_host"]), "ms_per_step": r["ms_host"],
