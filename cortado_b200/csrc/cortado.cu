@@ -583,20 +583,20 @@ __device__ __forceinline__ void client_apply(const OpArgs& A, long long c, int n
         }
       }
     }
-    // dequantized bins into the row
     const bool fast_i = __all_sync(0xffffffffu, bmax < 0x800000u);
-    __syncwarp();  // as above: the bins are read back from the row
+    if (OP == OP_S2C) {  // the request bins into the row
 #pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const uint4 b = (OP == OP_S2C) ? make_uint4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3])
-                                     : own[u ^ (tid & 7)];
-      own[u ^ (tid & 7)] = fast_i ? make_uint4(iq_fast(b.x, fq), iq_fast(b.y, fq), iq_fast(b.z, fq), iq_fast(b.w, fq))
-                                  : make_uint4(iq_mixed(b.x, fq, q), iq_mixed(b.y, fq, q), iq_mixed(b.z, fq, q),
-                                               iq_mixed(b.w, fq, q));
+      for (int u = 0; u < 8; u++) own[u ^ (tid & 7)] = make_uint4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
     }
-    __syncwarp();
+    __syncwarp();  // the warp's rows hold its bins
+    // dequantized on the way out, 512 contiguous bytes at a time
 #pragma unroll 2
-    for (int i = 0; i < 8; i++) g4[32 * i + lane] = *unit(i);
+    for (int i = 0; i < 8; i++) {
+      const uint4 b = *unit(i);
+      g4[32 * i + lane] = fast_i ? make_uint4(iq_fast(b.x, fq), iq_fast(b.y, fq), iq_fast(b.z, fq), iq_fast(b.w, fq))
+                                 : make_uint4(iq_mixed(b.x, fq, q), iq_mixed(b.y, fq, q), iq_mixed(b.z, fq, q),
+                                              iq_mixed(b.w, fq, q));
+    }
     __syncwarp();  // the rows are read before the encoder reuses the buffer
   } else {
     uint32_t* row = reinterpret_cast<uint32_t*>(A.client) + c * (long long)CW + 32 * tid;
