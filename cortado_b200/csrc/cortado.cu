@@ -18,9 +18,10 @@ using namespace cortado;
 // ================================================================== kernels
 // Resident CTAs per SM each kernel is compiled for (register budget
 // 65536 / (128 * n)); every kernel holds two 17 KiB buffers, so shared memory
-// allows 6.  resi_recv runs 5 (102 registers): at 80 its client and residual
-// words spill, and it measured 4.6% faster at 5; every other kernel measured
-// slower at 5 (and the store 10% slower with a third buffer at 4).
+// allows 6.  resi_recv runs 5 (a budget of 102 registers; it uses 96): at 80
+// its client and residual words spill, and it measured 4.6% faster at 5;
+// every other kernel measured slower at 5 (and the store 10% slower with a
+// third buffer at 4).
 #ifndef MINB_STORE
 #define MINB_STORE 6
 #endif
