@@ -878,19 +878,30 @@ def main():
     if extras and world == 1:
         from cortado_b200.ops import Codec
         dev = torch.device("cuda", 0)
+
+        def extra(key, fn):
+            # a failing configuration is reported in its key; the line (and
+            # the measured flow above) still prints
+            try:
+                line[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+
+        def with_codec(fn):
+            c = Codec(0)
+            try:
+                return fn(c)
+            finally:
+                c.close()
+
         if "batched" in extras:
-            c = Codec(0)
-            line["batched"] = bench_batched(c, dev, n_fields=args.batched_fields, max_mb=args.batched_max_mb)
-            c.close()
-            torch.cuda.empty_cache()
+            extra("batched", lambda: with_codec(
+                lambda c: bench_batched(c, dev, n_fields=args.batched_fields, max_mb=args.batched_max_mb)))
         if "serving" in extras:
-            line["serving"] = bench_serving(dev)
-            torch.cuda.empty_cache()
+            extra("serving", lambda: bench_serving(dev))
         if "chain" in extras:
-            c = Codec(0)
-            line["chain"] = bench_chain(c, dev)
-            c.close()
-            torch.cuda.empty_cache()
+            extra("chain", lambda: with_codec(lambda c: bench_chain(c, dev)))
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(r["x_host"])
     print(json.dumps(line))
